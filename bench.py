@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""Benchmark: Msamples/s of the wavefront path tracer on one config.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl wrk|reference] [--config showcase]
+
+A step renders the whole workload (default: the material-showcase scene,
+512x512 at 256 spp, max depth 16) from a resident scene into device memory.
+With N > 1 (one process per GPU, launched by torch.distributed.run) every rank
+renders its own sample range of the image (weak scaling: the image gets N*spp
+samples) and the per-rank frames are summed with one NCCL all-reduce per step,
+the frame combine of a sample-split render.
+
+``value`` = all ranks' samples / max-over-ranks device time of the K timed steps.
+``e2e`` = the same metric through the public C ABI call with host output
+buffers (device->host copy of rgb, albedo and normal inside the timed region).
+``roofline`` is for the dominant kernel (extension-ray traversal); ``cpu_baseline``
+times the reference's own shading code compiled on the host (oracle/_ref),
+driven with OpenMP on all host cores, on a bounded sample of the same workload.
+``--impl reference`` runs that CPU implementation as the reference arm.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from offlinerenderer_b200 import scenes  # noqa: E402
+
+CONFIGS = {
+    "showcase": dict(make=lambda: scenes.material_showcase(512, 512, 256, seed=1),
+                     workload="material_showcase 512x512 256spp maxDepth16 (Cornell room + 3 icospheres subdiv 4, "
+                              "15372 tris, 1024^2 checker albedo + value-noise normal map)"),
+    "cornell": dict(make=lambda: scenes.cornell(256, 256, 64, seed=1),
+                    workload="cornell 256x256 64spp maxDepth8 (36 tris)"),
+    "scale": dict(make=lambda: scenes.scale_test(1920, 1080, 64, seed=1),
+                  workload="scale_test 1920x1080 64spp maxDepth8 (fBm heightfield 1024^2 + 250 icospheres, ~2.41M tris)"),
+}
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+# Algorithmic bytes per extension ray for the trace kernel: read the ray
+# (origin|tmin, direction|tmax = 32 B) + write the hit record (t, prim, material = 16 B).
+TRACE_BYTES_PER_RAY = 48
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def hbm_peak():
+    try:
+        d = json.load(open(MEASURED_PEAKS))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def cpu_reference_rate(sd, threads: int, target_s: float = 12.0):
+    """Reference shading code on the host cores (oracle/_ref), bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    kind = "reference"
+    try:
+        eng = pyoracle.Reference()
+    except FileNotFoundError:
+        pyoracle.build()
+        eng, kind = pyoracle.Oracle(), "port"
+    sc = eng.scene(sd)
+    st = sd.settings
+    rows = max(1, st.height // 16)
+    t0 = time.perf_counter()
+    _, _, _, s1 = sc.render(spp=1, threads=threads, pixel_begin=0, pixel_end=rows * st.width)
+    dt = time.perf_counter() - t0
+    spp = int(max(1, min(st.spp, target_s / max(dt, 1e-3) / 16)))
+    t0 = time.perf_counter()
+    _, _, _, s2 = sc.render(spp=spp, threads=threads)
+    dt = time.perf_counter() - t0
+    samples = st.width * st.height * spp
+    return {"value": samples / dt / 1e6, "unit": "Msamples/s", "cores": threads, "kind": kind,
+            "sample": f"{st.width}x{st.height} at {spp} spp of the same scene and settings ({samples} samples, "
+                      f"{dt:.1f} s)",
+            "mrays_per_s": (s2["extension_rays"] + s2["shadow_rays"]) / dt / 1e6}
+
+
+def run_reference_arm(args, cfg):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    sd = cfg["make"]()
+    threads = os.cpu_count() or 1
+    kind = "reference"
+    try:
+        eng = pyoracle.Reference()
+    except FileNotFoundError:
+        pyoracle.build()
+        eng, kind = pyoracle.Oracle(), "port"
+    sc = eng.scene(sd)
+    st = sd.settings
+    # each step: every pixel at 1 spp (a bounded sample of the workload)
+    for i in range(args.warmup):
+        sc.render(spp=1, threads=threads, sample_begin=i)
+    t0 = time.perf_counter()
+    rays = 0
+    for i in range(args.steps):
+        _, _, _, s = sc.render(spp=1, threads=threads, sample_begin=args.warmup + i)
+        rays += s["extension_rays"] + s["shadow_rays"]
+    dt = time.perf_counter() - t0
+    samples = st.width * st.height * args.steps
+    v = samples / dt / 1e6
+    out = {"impl": "reference", "metric": "Msamples/s", "value": v, "unit": "Msamples/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+           "config": {"workload": cfg["workload"], "step": f"{st.width}x{st.height} at 1 spp on the host cores"},
+           "cpu_baseline": {"value": v, "unit": "Msamples/s", "cores": threads, "kind": kind,
+                            "sample": f"{args.steps} steps of {st.width}x{st.height} at 1 spp"},
+           "e2e": {"value": v, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "mrays_per_s": rays / dt / 1e6}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="wrk", choices=["wrk", "reference"])
+    ap.add_argument("--config", default="showcase", choices=list(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference_arm(args, cfg)
+        return
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from offlinerenderer_b200 import build as _b
+    from offlinerenderer_b200 import wrk
+
+    _b.build()
+    sd = cfg["make"]()
+    st = sd.settings
+    scene = wrk.Scene.from_data(sd, device=local)
+    rend = wrk.Renderer(device=local)
+    npx = st.width * st.height
+    frame = torch.zeros(npx * 3, dtype=torch.float32, device=f"cuda:{local}")
+    samples_per_step = npx * st.spp
+
+    def step(i):
+        off = (i * world + rank) * st.spp
+        s = rend.render_device(scene, None, d_rgb_ptr=frame.data_ptr(), sample_offset=off)
+        if dist is not None:
+            dist.all_reduce(frame)  # combine the ranks' sample ranges
+        return s
+
+    for i in range(args.warmup):
+        step(i)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    iters = 0
+    rays = 0
+    for i in range(args.steps):
+        s = step(args.warmup + i)
+        iters += s["iterations"]
+        rays += s["extensionRays"] + s["shadowRays"]
+    e1.record()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps * samples_per_step / (ms / 1e3) / 1e6
+    mrays = world * rays / (ms / 1e3) / 1e6
+
+    # per-stage device times (events on the renderer's stream), one extra render
+    tst = rend.render_device(scene, None, d_rgb_ptr=frame.data_ptr(), stage_timing=True)
+    stage_ms = tst["stageMs"]
+    dominant = max(stage_ms, key=lambda k: stage_ms[k])
+    tr_ms = stage_ms["trace_extension"]
+    tr_launches = max(1, tst["stageLaunches"]["trace_extension"])
+    tr_bytes = TRACE_BYTES_PER_RAY * tst["extensionRays"]
+    peak, peak_kind = hbm_peak()
+    achieved = tr_bytes / (tr_ms / 1e3) / 1e9 if tr_ms > 0 else None
+
+    # end to end through the public C ABI with host buffers
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record()
+    for i in range(e2e_steps):
+        rend.render(scene, sample_offset=(1000 + i * world + rank) * st.spp)
+    e3.record()
+    torch.cuda.synchronize()
+    e2e_ms = e2.elapsed_time(e3)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_val = world * e2e_steps * samples_per_step / (e2e_ms / 1e3) / 1e6
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_rate(sd, os.cpu_count() or 1)
+
+    if rank == 0:
+        out = {
+            "metric": "Msamples/s",
+            "value": value,
+            "unit": "Msamples/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded procedural scene; no dataset)",
+            "config": {"workload": cfg["workload"], "samples_per_step_per_gpu": samples_per_step,
+                       "parallelism": f"sample-split x{world}, one NCCL all-reduce of the frame per step"
+                       if world > 1 else "single GPU",
+                       "l2": "per-step working set (path slots 4M x 144 B = 604 MB) exceeds the 126 MB L2"},
+            "mrays_per_s": mrays,
+            "iterations_per_step": iters / args.steps,
+            "gpu_launches": iters * 8 + args.steps * 2,
+            "e2e": {"value": e2e_val, "unit": "Msamples/s", "h2d_bytes_per_step": 76 + 44,
+                    "d2h_bytes_per_step": npx * 3 * 4 * 3},
+            "roofline": {"bound": "hbm", "kernel": "k_trace_extension", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "peak_source": peak_kind, "avg_launch_ms": tr_ms / tr_launches,
+                         "algorithmic_bytes_per_launch": tr_bytes / tr_launches, "dominant_stage": dominant},
+            "stage_ms": stage_ms,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    del frame
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

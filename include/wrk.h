@@ -1,0 +1,191 @@
+/* wrk.h -- C ABI of the B200 wavefront path tracer (libwrk.so).
+ *
+ * Plain C: opaque handles, POD structs, pointers and sizes; every call returns
+ * an int status (WRK_OK = 0) and wrk_last_error() gives the message of the last
+ * failure on the calling thread.  No exception crosses this boundary; the C++
+ * layer (include/wr/*.h) rethrows failures as std::runtime_error, the error
+ * convention of libWR's CUDA_CHECK / CU_CHECK macros
+ * (libWR/src/internal/cuda_utils.h:13-39).
+ *
+ * Each entry point names the libWR interface it replaces
+ * (paths inside trianglestrip/OfflineRenderer).
+ */
+#ifndef WRK_H
+#define WRK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    WRK_OK = 0,
+    WRK_ERR_INVALID = 1,   /* bad argument or size */
+    WRK_ERR_CUDA = 2,      /* CUDA runtime failure */
+    WRK_ERR_STATE = 3,     /* call out of order (e.g. render before finalize) */
+    WRK_ERR_NO_DEVICE = 4, /* no CUDA device / extension unusable */
+    WRK_ERR_DEVICE = 5     /* a kernel reported an internal error (stack overflow, bad index) */
+};
+
+enum { WRK_LAMBERTIAN = 0, WRK_EMISSIVE = 1, WRK_GLASS = 2, WRK_GGX_REFLECTION = 3, WRK_GGX_TRANSMISSION = 4 };
+
+/* 64-byte material record; field meaning of MaterialData
+ * (libWR/src/internal/gpu_types.h:28-37). */
+typedef struct {
+    float albedo[4];
+    float emission[4];
+    float ior;
+    uint32_t type;
+    float roughness;
+    float metallic;
+    uint32_t albedoTextureId; /* 1-based texture id, 0 = constant albedo */
+    uint32_t normalTextureId; /* 1-based texture id, 0 = no normal map */
+    uint32_t pad[2];
+} wrk_material;
+
+/* wr::Camera (libWR/include/wr/types.h:16-51); fovY in radians, vertical. */
+typedef struct {
+    float position[3], target[3], up[3];
+    float fovY, aspect, focalDistance, lensRadius;
+} wrk_camera;
+
+/* wr::RenderParams (libWR/include/wr/renderer.h:25-36) plus additive fields. */
+typedef struct {
+    uint32_t width, height, spp;
+    uint32_t useNEE;
+    uint32_t maxBounces;
+    float russianRouletteDepth;
+    float fireflyClamp;
+    uint32_t seed;          /* 0 = the reference's per-pixel seed formula (trace.cu:58) */
+    uint32_t maxIterations; /* wavefront iterations a path may use; 0 = 8, the reference host loop's cap (renderer.cpp:213) */
+    uint32_t flags;         /* WRK_FLAG_* */
+    uint32_t sampleOffset;  /* render sample indices [sampleOffset, sampleOffset+spp): splits one image across calls / GPUs */
+} wrk_render_params;
+
+/* Guides (albedo / normal) are returned averaged over spp; with this flag they
+ * are the raw per-pixel sums libWR keeps (trace.cu:277-283). */
+#define WRK_FLAG_RAW_GUIDES 1u
+/* Record CUDA events around every kernel of the loop (on the renderer's stream)
+ * and report per-stage device time in wrk_render_stats.stageMs. */
+#define WRK_FLAG_STAGE_TIMING 2u
+
+enum {
+    WRK_STAGE_CONTROL = 0,
+    WRK_STAGE_GENERATE = 1,
+    WRK_STAGE_TRACE_EXTENSION = 2,
+    WRK_STAGE_TRACE_SHADOW = 3,
+    WRK_STAGE_SHADE_LAMBERT = 4,
+    WRK_STAGE_SHADE_DIELECTRIC = 5,
+    WRK_STAGE_SHADE_GGX = 6,
+    WRK_STAGE_SHADE_EMISSIVE = 7,
+    WRK_NUM_STAGES = 8
+};
+
+typedef struct {
+    uint64_t paths;          /* camera paths started */
+    uint64_t extensionRays;  /* closest-hit rays traced */
+    uint64_t shadowRays;     /* any-hit rays traced */
+    uint32_t iterations;     /* wavefront iterations issued */
+    uint32_t deviceErrors;   /* internal device error flags raised (0 = none) */
+    float gpuMs;             /* device time of the render loop (CUDA events) */
+    float totalMs;           /* device time including uploads / readback */
+    float stageMs[8];        /* per-stage device time (WRK_FLAG_STAGE_TIMING), indexed by WRK_STAGE_* */
+    uint32_t stageLaunches[8];
+} wrk_render_stats;
+
+typedef struct {
+    uint32_t numTriangles;
+    uint32_t numNodes;     /* 8-wide BVH nodes (80 bytes each) */
+    uint32_t numBinaryNodes;
+    uint32_t depth;        /* 8-wide depth */
+    uint32_t numEmissive;
+    float buildMs;         /* GPU time of the BVH build */
+    float sahCost;         /* SAH cost of the 8-wide tree (node visits + triangle tests per ray, area-weighted) */
+} wrk_bvh_info;
+
+typedef struct wrk_scene wrk_scene;
+typedef struct wrk_renderer wrk_renderer;
+
+const char* wrk_last_error(void);
+int wrk_version(void);
+
+/* ---- device memory helpers (for callers without their own allocator) ---- */
+int wrk_device_count(int* count);
+int wrk_malloc(int device, uint64_t bytes, void** ptr);
+int wrk_free(void* ptr);
+int wrk_memcpy_htod(void* dst, const void* src, uint64_t bytes);
+int wrk_memcpy_dtoh(void* dst, const void* src, uint64_t bytes);
+int wrk_synchronize(int device);
+
+/* ---- scene: replaces wr::Scene (libWR/include/wr/scene.h:33-101,
+ *      libWR/src/internal/scene.cpp:91-557) ---- */
+int wrk_scene_create(int device, wrk_scene** out);
+int wrk_scene_destroy(wrk_scene* s);
+/* Flat triangle soup as Scene::addTriangleMesh accumulates it (scene.cpp:190-244):
+ * vertices 3 floats each; normals (3 each) and uvs (2 each) may be NULL. */
+int wrk_scene_set_geometry(wrk_scene* s, const float* vertices, uint32_t numVertices, const float* normals,
+                           const float* uvs, const uint32_t* indices, uint32_t numTriangles,
+                           const uint32_t* triMaterial);
+int wrk_scene_set_materials(wrk_scene* s, const wrk_material* materials, uint32_t numMaterials);
+/* RGBA8 texture (Scene::loadTexture, scene.cpp:246-264); returns the 1-based id. */
+int wrk_scene_add_texture(wrk_scene* s, const uint8_t* rgba, uint32_t width, uint32_t height, uint32_t* outId);
+int wrk_scene_set_environment(wrk_scene* s, const float rgb[3]);
+/* Scene::finalize (scene.cpp:350-557): uploads, builds the emissive list and power
+ * CDF (same serial FP32 order as scene.cpp:423-491), builds the 8-wide BVH on the GPU
+ * (replaces optixAccelBuild, scene.cpp:493-550). */
+int wrk_scene_finalize(wrk_scene* s);
+int wrk_scene_bvh_info(wrk_scene* s, wrk_bvh_info* info);
+/* Light list / CDF readback (getEmissiveTrianglesBuffer, getEmissiveTriangleCDFBuffer). */
+int wrk_scene_light_cdf(wrk_scene* s, uint32_t* tris, float* cdf, uint32_t capacity, uint32_t* count);
+
+/* Device addresses of a finalized scene's buffers: the getters of wr::Scene
+ * (libWR/include/wr/scene.h:70-93); bvhNodes stands in for the GAS handle. */
+typedef struct {
+    uint64_t vertices, normals, uvs, indices, triMaterial, materials, emissive, cdf, texels, bvhNodes, bvhTriangles;
+    uint32_t numMaterials, numEmissive, numTextures, numTriangles;
+} wrk_scene_buffers;
+int wrk_scene_buffers_get(wrk_scene* s, wrk_scene_buffers* out);
+
+/* ---- renderer: replaces wr::Renderer::render (libWR/src/internal/renderer.cpp:132-316) ---- */
+/* capacity = path slots in flight (0 = chosen from the device). */
+int wrk_renderer_create(int device, uint32_t capacity, wrk_renderer** out);
+int wrk_renderer_destroy(wrk_renderer* r);
+/* Synchronous render into HOST buffers of width*height*3 floats: rgb = sum/spp
+ * (renderer.cpp:308-313), albedo / normal first-hit guides (may be NULL). */
+int wrk_render(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, const wrk_render_params* p, float* rgb,
+               float* albedo, float* normal, wrk_render_stats* stats);
+/* Same render into DEVICE buffers (float3 per pixel), enqueued on the renderer's
+ * stream; the call returns after the loop has finished on the device. */
+int wrk_render_device(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, const wrk_render_params* p, float* d_rgb,
+                      float* d_albedo, float* d_normal, wrk_render_stats* stats);
+
+/* ---- kernel-level entry points (device pointers; synchronous) ---- */
+/* Closest hit (optixTrace + __closesthit__trace, trace.cu:127-141):
+ * rays = 8 floats each (ox,oy,oz,tmin,dx,dy,dz,tmax); t = +inf and prim = 0xffffffff on miss. */
+int wrk_trace_closest(wrk_scene* s, const float* d_rays, uint32_t n, float* d_t, uint32_t* d_prim);
+/* Visibility (the Shadow stage of __raygen__trace, trace.cu:27-51): 1 = occluded. */
+int wrk_trace_occluded(wrk_scene* s, const float* d_rays, uint32_t n, uint32_t* d_occluded);
+/* Stable compaction (compact.cu:6-17): keeps idxIn[i] whose stage[idxIn[i]] != 3,
+ * in input order; *d_count receives the survivor count. */
+int wrk_compact(const uint32_t* d_stage, const uint32_t* d_idxIn, uint32_t n, uint32_t* d_idxOut, uint32_t* d_count);
+/* Light selection (sampleEmissiveTriangle, sampling.cuh:116-135). */
+int wrk_cdf_sample(const float* d_cdf, uint32_t ncdf, const float* d_u, uint32_t n, uint32_t* d_out);
+/* PCG hash with dimension and its uniform (sampling.cuh:24-38). */
+int wrk_rng_batch(const uint32_t* d_seed, const uint32_t* d_dim, uint32_t n, uint32_t* d_hash, float* d_u);
+/* BSDF / sampling math on the device for batches of records (20 floats in, 34 out):
+ * GGX eval/pdf/VNDF sample, dielectric Fresnel, cosine warp, MIS power heuristic,
+ * Russian roulette, frames, triangle sampling, shading correction. */
+int wrk_bsdf_batch(const float* d_in, uint32_t n, float* d_out);
+/* Bilinear RGBA8 texture fetch (wrap, normalized float) of texture id of a finalized scene. */
+int wrk_texture_batch(wrk_scene* s, uint32_t textureId, const float* d_uv, uint32_t n, float* d_out);
+/* Camera rays for (pixel, sample) pairs (the depth-0 branch of __raygen__trace). */
+int wrk_camera_rays(const wrk_camera* cam, uint32_t width, uint32_t height, const uint32_t* d_pixels,
+                    const uint32_t* d_samples, uint32_t n, uint32_t seed, float* d_rays);
+/* Exposure 2.2, ACES filmic fit, gamma 1/2.2, 8-bit (libWR/test/helpers/image.cpp:14-49). */
+int wrk_tonemap_aces(const float* d_rgb, uint32_t numPixels, uint8_t* d_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WRK_H */

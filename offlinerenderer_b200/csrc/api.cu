@@ -1,0 +1,694 @@
+// C ABI of libwrk (include/wrk.h): scene upload and BVH build, the renderer's
+// host loop, and the kernel-level entry points.  Errors are returned as codes with
+// a per-thread message (wrk_last_error); no exception crosses the boundary.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "wrk_internal.h"
+
+namespace wrk {
+int compact_stable(const uint32_t* stage, const uint32_t* idx, uint32_t n, uint32_t* out, uint32_t* count,
+                   cudaStream_t st);
+void launch_cdf(const float* cdf, uint32_t ncdf, const float* u, uint32_t n, uint32_t* out, cudaStream_t st);
+void launch_rng(const uint32_t* s, const uint32_t* d, uint32_t n, uint32_t* h, float* u, cudaStream_t st);
+void launch_bsdf(const float* in, uint32_t n, float* out, cudaStream_t st);
+void launch_texture(const uint8_t* texels, uint32_t w, uint32_t h, const float* uv, uint32_t n, float* out,
+                    cudaStream_t st);
+void launch_camera_rays(const Frame& f, const uint32_t* px, const uint32_t* sm, uint32_t n, float* out,
+                        cudaStream_t st);
+void launch_tonemap(const float* rgb, uint32_t nfloat, uint8_t* out, int grid, int vec, cudaStream_t st);
+}  // namespace wrk
+
+using namespace wrk;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(x)                                                                                          \
+    do {                                                                                               \
+        cudaError_t e_ = (x);                                                                          \
+        if (e_ != cudaSuccess) return fail(WRK_ERR_CUDA, "%s: %s (%s:%d)", #x, cudaGetErrorString(e_), \
+                                           __FILE__, __LINE__);                                        \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() { if (p) cudaFree(p); }
+    int alloc(size_t n) {
+        if (n <= bytes && p) return WRK_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        if (n == 0) return WRK_OK;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e != cudaSuccess) return fail(WRK_ERR_CUDA, "cudaMalloc(%zu): %s", n, cudaGetErrorString(e));
+        bytes = n;
+        return WRK_OK;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+int set_device(int dev) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(WRK_ERR_NO_DEVICE, "no CUDA device available");
+    if (dev < 0 || dev >= n) return fail(WRK_ERR_INVALID, "device %d out of range (%d devices)", dev, n);
+    CK(cudaSetDevice(dev));
+    return WRK_OK;
+}
+
+// Camera basis exactly as libWR computes it on the host: wr::Camera's GLM helpers
+// (libWR/include/wr/types.h:41-50; normalize = v * (1/sqrt(dot))) and
+// tan(fovY/2) (libWR/src/internal/renderer.cpp:144-156).
+void camera_frame(const wrk_camera& c, Frame& f) {
+    auto nrm = [](float v[3]) {
+        float r = 1.0f / std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        v[0] = v[0] * r;
+        v[1] = v[1] * r;
+        v[2] = v[2] * r;
+    };
+    auto crs = [](const float a[3], const float b[3], float o[3]) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    for (int k = 0; k < 3; ++k) {
+        f.pos[k] = c.position[k];
+        f.fwd[k] = c.target[k] - c.position[k];
+    }
+    nrm(f.fwd);
+    crs(f.fwd, c.up, f.right);
+    nrm(f.right);
+    crs(f.right, f.fwd, f.up);
+    nrm(f.up);
+    f.tanHalf = std::tan(c.fovY * 0.5f);
+    f.aspect = c.aspect;
+    f.focal = c.focalDistance;
+    f.lens = c.lensRadius;
+}
+
+}  // namespace
+
+struct wrk_scene {
+    int device = 0;
+    std::vector<float> vtx, nrm, uv;
+    std::vector<uint32_t> idx, triMat;
+    std::vector<wrk_material> mats;
+    std::vector<std::vector<uint8_t>> tex;
+    std::vector<uint32_t> texW, texH;
+    float env[3] = {0, 0, 0};
+    bool finalized = false;
+    DevBuf dVtx, dNrm, dUv, dIdx, dTriMat, dMats, dTexels, dTexInfo, dEmissive, dCdf, dErr;
+    uint4* nodes = nullptr;
+    float4* tris = nullptr;
+    std::vector<uint32_t> emissive;
+    std::vector<float> cdf;
+    wrk_bvh_info info{};
+    DevScene view{};
+    ~wrk_scene() {
+        cudaFree(nodes);
+        cudaFree(tris);
+    }
+};
+
+struct wrk_renderer {
+    int device = 0;
+    uint32_t capacity = 0;
+    int numSMs = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evLoop0 = nullptr, evLoop1 = nullptr;
+    std::vector<cudaEvent_t> stageEv;  // per-launch events for WRK_FLAG_STAGE_TIMING
+    DevBuf slots, queues, counters, frameBufs, outBufs;
+    Counters* hostCtr = nullptr;  // pinned
+    PathSoA soa{};
+    Queues q{};
+    ~wrk_renderer() {
+        if (hostCtr) cudaFreeHost(hostCtr);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (evLoop0) cudaEventDestroy(evLoop0);
+        if (evLoop1) cudaEventDestroy(evLoop1);
+        for (cudaEvent_t e : stageEv) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+__global__ void k_iota(uint32_t* a, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = i;
+}
+
+// Light list + power CDF exactly as Scene::finalize builds it
+// (libWR/src/internal/scene.cpp:423-491): serial FP32 over triangles in order.
+void build_light_cdf(wrk_scene* s) {
+    s->emissive.clear();
+    s->cdf.clear();
+    float total = 0.0f;
+    uint32_t nt = (uint32_t)s->triMat.size();
+    for (uint32_t t = 0; t < nt; ++t) {
+        uint32_t m = s->triMat[t];
+        if (m >= s->mats.size() || s->mats[m].type != WRK_EMISSIVE) continue;
+        s->emissive.push_back(t);
+        const float* a = &s->vtx[3 * (size_t)s->idx[3 * t]];
+        const float* b = &s->vtx[3 * (size_t)s->idx[3 * t + 1]];
+        const float* c = &s->vtx[3 * (size_t)s->idx[3 * t + 2]];
+        float e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]}, e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+        float cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        float area = 0.5f * std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+        const wrk_material& mm = s->mats[m];
+        float power = (mm.emission[0] + mm.emission[1] + mm.emission[2]) * area;
+        total += power;
+        s->cdf.push_back(total);
+    }
+    for (float& c : s->cdf) c /= total;
+}
+
+template <class T>
+int upload(DevBuf& b, const std::vector<T>& v) {
+    if (v.empty()) return WRK_OK;
+    int rc = b.alloc(sizeof(T) * v.size());
+    if (rc) return rc;
+    CK(cudaMemcpy(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+    return WRK_OK;
+}
+
+int check_scene(wrk_scene* s) {
+    if (!s) return fail(WRK_ERR_INVALID, "null scene");
+    if (!s->finalized) return fail(WRK_ERR_STATE, "scene not finalized");
+    return set_device(s->device);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* wrk_last_error(void) { return g_err.c_str(); }
+int wrk_version(void) { return 1; }
+
+int wrk_device_count(int* count) {
+    if (!count) return fail(WRK_ERR_INVALID, "null count");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    *count = e == cudaSuccess ? n : 0;
+    return WRK_OK;
+}
+int wrk_malloc(int device, uint64_t bytes, void** ptr) {
+    if (!ptr) return fail(WRK_ERR_INVALID, "null ptr");
+    int rc = set_device(device);
+    if (rc) return rc;
+    CK(cudaMalloc(ptr, bytes ? bytes : 1));
+    return WRK_OK;
+}
+int wrk_free(void* ptr) {
+    CK(cudaFree(ptr));
+    return WRK_OK;
+}
+int wrk_memcpy_htod(void* dst, const void* src, uint64_t bytes) {
+    CK(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    return WRK_OK;
+}
+int wrk_memcpy_dtoh(void* dst, const void* src, uint64_t bytes) {
+    CK(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+    return WRK_OK;
+}
+int wrk_synchronize(int device) {
+    int rc = set_device(device);
+    if (rc) return rc;
+    CK(cudaDeviceSynchronize());
+    return WRK_OK;
+}
+
+// ---------------------------------------------------------------------------
+int wrk_scene_create(int device, wrk_scene** out) {
+    if (!out) return fail(WRK_ERR_INVALID, "null out");
+    int rc = set_device(device);
+    if (rc) return rc;
+    wrk_scene* s = new wrk_scene();
+    s->device = device;
+    *out = s;
+    return WRK_OK;
+}
+int wrk_scene_destroy(wrk_scene* s) {
+    if (s) {
+        cudaSetDevice(s->device);
+        delete s;
+    }
+    return WRK_OK;
+}
+int wrk_scene_set_geometry(wrk_scene* s, const float* vertices, uint32_t nv, const float* normals, const float* uvs,
+                           const uint32_t* indices, uint32_t nt, const uint32_t* triMaterial) {
+    if (!s || !vertices || !indices || !triMaterial) return fail(WRK_ERR_INVALID, "null geometry argument");
+    if (s->finalized) return fail(WRK_ERR_STATE, "scene already finalized");
+    if (nv == 0 || nt == 0) return fail(WRK_ERR_INVALID, "Scene has no geometry");
+    for (size_t i = 0; i < 3 * (size_t)nt; ++i)
+        if (indices[i] >= nv) return fail(WRK_ERR_INVALID, "index %u out of range (vertex count %u)", indices[i], nv);
+    s->vtx.assign(vertices, vertices + 3 * (size_t)nv);
+    s->nrm.clear();
+    s->uv.clear();
+    if (normals) s->nrm.assign(normals, normals + 3 * (size_t)nv);
+    if (uvs) s->uv.assign(uvs, uvs + 2 * (size_t)nv);
+    s->idx.assign(indices, indices + 3 * (size_t)nt);
+    s->triMat.assign(triMaterial, triMaterial + nt);
+    return WRK_OK;
+}
+int wrk_scene_set_materials(wrk_scene* s, const wrk_material* m, uint32_t n) {
+    if (!s || (!m && n)) return fail(WRK_ERR_INVALID, "null materials");
+    if (s->finalized) return fail(WRK_ERR_STATE, "scene already finalized");
+    s->mats.assign(m, m + n);
+    return WRK_OK;
+}
+int wrk_scene_add_texture(wrk_scene* s, const uint8_t* rgba, uint32_t w, uint32_t h, uint32_t* outId) {
+    if (!s || !rgba || !outId || w == 0 || h == 0) return fail(WRK_ERR_INVALID, "bad texture arguments");
+    if (s->finalized) return fail(WRK_ERR_STATE, "scene already finalized");
+    s->tex.emplace_back(rgba, rgba + 4 * (size_t)w * h);
+    s->texW.push_back(w);
+    s->texH.push_back(h);
+    *outId = (uint32_t)s->tex.size();
+    return WRK_OK;
+}
+int wrk_scene_set_environment(wrk_scene* s, const float rgb[3]) {
+    if (!s || !rgb) return fail(WRK_ERR_INVALID, "null environment");
+    for (int k = 0; k < 3; ++k) s->env[k] = rgb[k];
+    s->view.env[0] = rgb[0];
+    s->view.env[1] = rgb[1];
+    s->view.env[2] = rgb[2];
+    return WRK_OK;
+}
+
+int wrk_scene_finalize(wrk_scene* s) {
+    if (!s) return fail(WRK_ERR_INVALID, "null scene");
+    if (s->finalized) return WRK_OK;  // as Scene::finalize (scene.cpp:351)
+    if (s->vtx.empty() || s->idx.empty()) return fail(WRK_ERR_INVALID, "Scene has no geometry");
+    int rc = set_device(s->device);
+    if (rc) return rc;
+    uint32_t nt = (uint32_t)s->triMat.size();
+    build_light_cdf(s);
+    if ((rc = upload(s->dVtx, s->vtx)) || (rc = upload(s->dNrm, s->nrm)) || (rc = upload(s->dUv, s->uv)) ||
+        (rc = upload(s->dIdx, s->idx)) || (rc = upload(s->dTriMat, s->triMat)) || (rc = upload(s->dMats, s->mats)) ||
+        (rc = upload(s->dEmissive, s->emissive)) || (rc = upload(s->dCdf, s->cdf)))
+        return rc;
+    // texel pool + per-texture info
+    std::vector<TexInfo> ti;
+    size_t total = 0;
+    for (size_t i = 0; i < s->tex.size(); ++i) {
+        ti.push_back(TexInfo{total, s->texW[i], s->texH[i]});
+        total += (s->tex[i].size() + 15) & ~size_t(15);
+    }
+    if (!s->tex.empty()) {
+        if ((rc = s->dTexels.alloc(total))) return rc;
+        for (size_t i = 0; i < s->tex.size(); ++i)
+            CK(cudaMemcpy(s->dTexels.as<uint8_t>() + ti[i].offset, s->tex[i].data(), s->tex[i].size(),
+                          cudaMemcpyHostToDevice));
+        if ((rc = upload(s->dTexInfo, ti))) return rc;
+    }
+    if ((rc = s->dErr.alloc(sizeof(uint32_t)))) return rc;
+    BvhBuildResult br{};
+    char err[256] = {0};
+    rc = build_bvh8(s->dVtx.as<float>(), s->dIdx.as<uint32_t>(), s->dTriMat.as<uint32_t>(), nt, 0, &br, err,
+                    sizeof(err));
+    if (rc) return fail(rc, "%s", err);
+    s->nodes = br.nodes;
+    s->tris = br.tris;
+    s->info.numTriangles = nt;
+    s->info.numNodes = br.numNodes;
+    s->info.numBinaryNodes = br.numBinary;
+    s->info.depth = br.depth;
+    s->info.numEmissive = (uint32_t)s->emissive.size();
+    s->info.buildMs = br.ms;
+    s->info.sahCost = br.sah;
+    DevScene& v = s->view;
+    v.vtx = s->dVtx.as<float>();
+    v.nrm = s->nrm.empty() ? nullptr : s->dNrm.as<float>();
+    v.uv = s->uv.empty() ? nullptr : s->dUv.as<float>();
+    v.idx = s->dIdx.as<uint32_t>();
+    v.triMat = s->dTriMat.as<uint32_t>();
+    v.mats = s->dMats.as<wrk_material>();
+    v.numMats = (uint32_t)s->mats.size();
+    v.texels = s->dTexels.as<uint8_t>();
+    v.tex = s->dTexInfo.as<TexInfo>();
+    v.numTex = (uint32_t)s->tex.size();
+    v.emissive = s->dEmissive.as<uint32_t>();
+    v.cdf = s->dCdf.as<float>();
+    v.numEmissive = (uint32_t)s->emissive.size();
+    v.numTris = nt;
+    for (int k = 0; k < 3; ++k) v.env[k] = s->env[k];
+    v.nodes = s->nodes;
+    v.tris = s->tris;
+    v.numNodes = br.numNodes;
+    s->finalized = true;
+    return WRK_OK;
+}
+
+int wrk_scene_bvh_info(wrk_scene* s, wrk_bvh_info* info) {
+    int rc = check_scene(s);
+    if (rc) return rc;
+    if (!info) return fail(WRK_ERR_INVALID, "null info");
+    *info = s->info;
+    return WRK_OK;
+}
+
+int wrk_scene_light_cdf(wrk_scene* s, uint32_t* tris, float* cdf, uint32_t capacity, uint32_t* count) {
+    int rc = check_scene(s);
+    if (rc) return rc;
+    uint32_t n = (uint32_t)s->emissive.size();
+    if (count) *count = n;
+    if (n > capacity) return fail(WRK_ERR_INVALID, "capacity %u < %u emissive triangles", capacity, n);
+    if (n) {
+        // read back what the device holds
+        if (tris) CK(cudaMemcpy(tris, s->dEmissive.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+        if (cdf) CK(cudaMemcpy(cdf, s->dCdf.p, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    }
+    return WRK_OK;
+}
+
+int wrk_scene_buffers_get(wrk_scene* s, wrk_scene_buffers* o) {
+    int rc = check_scene(s);
+    if (rc) return rc;
+    if (!o) return fail(WRK_ERR_INVALID, "null out");
+    const DevScene& v = s->view;
+    o->vertices = (uint64_t)(uintptr_t)v.vtx;
+    o->normals = (uint64_t)(uintptr_t)v.nrm;
+    o->uvs = (uint64_t)(uintptr_t)v.uv;
+    o->indices = (uint64_t)(uintptr_t)v.idx;
+    o->triMaterial = (uint64_t)(uintptr_t)v.triMat;
+    o->materials = (uint64_t)(uintptr_t)v.mats;
+    o->emissive = (uint64_t)(uintptr_t)v.emissive;
+    o->cdf = (uint64_t)(uintptr_t)v.cdf;
+    o->texels = (uint64_t)(uintptr_t)v.texels;
+    o->bvhNodes = (uint64_t)(uintptr_t)v.nodes;
+    o->bvhTriangles = (uint64_t)(uintptr_t)v.tris;
+    o->numMaterials = v.numMats;
+    o->numEmissive = v.numEmissive;
+    o->numTextures = v.numTex;
+    o->numTriangles = v.numTris;
+    return WRK_OK;
+}
+
+// ---------------------------------------------------------------------------
+int wrk_renderer_create(int device, uint32_t capacity, wrk_renderer** out) {
+    if (!out) return fail(WRK_ERR_INVALID, "null out");
+    int rc = set_device(device);
+    if (rc) return rc;
+    wrk_renderer* r = new wrk_renderer();
+    r->device = device;
+    cudaDeviceGetAttribute(&r->numSMs, cudaDevAttrMultiProcessorCount, device);
+    if (capacity == 0) capacity = 1u << 22;
+    capacity = std::max(capacity, 1024u);
+    r->capacity = capacity;
+    auto bail = [&](int code) {
+        delete r;
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess ||
+        cudaEventCreate(&r->evLoop0) != cudaSuccess || cudaEventCreate(&r->evLoop1) != cudaSuccess)
+        return bail(fail(WRK_ERR_CUDA, "stream/event creation failed"));
+    if (cudaMallocHost(&r->hostCtr, sizeof(Counters)) != cudaSuccess)
+        return bail(fail(WRK_ERR_CUDA, "pinned counter allocation failed"));
+    size_t C = capacity;
+    if ((rc = r->slots.alloc(C * (8 * sizeof(float4) + sizeof(uint4))))) return bail(rc);
+    float4* base = r->slots.as<float4>();
+    r->soa.ray_o = base;
+    r->soa.ray_d = base + C;
+    r->soa.hit = base + 2 * C;
+    r->soa.thr = base + 3 * C;
+    r->soa.rad = base + 4 * C;
+    r->soa.sh_o = base + 5 * C;
+    r->soa.sh_d = base + 6 * C;
+    r->soa.sh_c = base + 7 * C;
+    r->soa.st = reinterpret_cast<uint4*>(base + 8 * C);
+    if ((rc = r->queues.alloc(C * sizeof(uint32_t) * (4 + kNumBuckets + 1)))) return bail(rc);
+    uint32_t* qb = r->queues.as<uint32_t>();
+    r->q.ext[0] = qb;
+    r->q.ext[1] = qb + C;
+    r->q.shd[0] = qb + 2 * C;
+    r->q.shd[1] = qb + 3 * C;
+    for (int b = 0; b < kNumBuckets; ++b) r->q.bucket[b] = qb + (4 + b) * C;
+    r->q.freeStack = qb + (4 + kNumBuckets) * C;
+    if ((rc = r->counters.alloc(sizeof(Counters)))) return bail(rc);
+    r->q.ctr = r->counters.as<Counters>();
+    r->q.capacity = capacity;
+    *out = r;
+    return WRK_OK;
+}
+
+int wrk_renderer_destroy(wrk_renderer* r) {
+    if (r) {
+        cudaSetDevice(r->device);
+        cudaStreamSynchronize(r->stream);
+        delete r;
+    }
+    return WRK_OK;
+}
+
+static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, const wrk_render_params* p, float* d_rgb,
+                       float* d_alb, float* d_nrm, wrk_render_stats* stats) {
+    Frame f{};
+    camera_frame(*cam, f);
+    f.width = p->width;
+    f.height = p->height;
+    f.spp = p->spp;
+    f.useNEE = p->useNEE ? 1u : 0u;
+    f.maxBounces = p->maxBounces;
+    f.seed = p->seed;
+    f.sampleOffset = p->sampleOffset;
+    f.maxIter = p->maxIterations ? p->maxIterations : 8u;
+    f.rrStart = p->russianRouletteDepth;
+    f.fireflyClamp = p->fireflyClamp;
+    f.tilesX = (p->width % 8 == 0 && p->height % 4 == 0) ? p->width / 8 : 0;
+    f.perSample = p->width * p->height;
+    size_t np = (size_t)p->width * p->height;
+    int rc = r->frameBufs.alloc(np * 3 * sizeof(float4));
+    if (rc) return rc;
+    f.accum = r->frameBufs.as<float4>();
+    f.albedo = f.accum + np;
+    f.normal = f.albedo + np;
+    f.err = &r->q.ctr->error;
+    cudaStream_t st = r->stream;
+    CK(cudaEventRecord(r->ev0, st));
+    CK(cudaMemsetAsync(f.accum, 0, np * 3 * sizeof(float4), st));
+    Counters c0{};
+    c0.cur = 1;
+    c0.freeCount = r->capacity;
+    c0.totalWork = (unsigned long long)np * p->spp;
+    CK(cudaMemcpyAsync(r->q.ctr, &c0, sizeof(Counters), cudaMemcpyHostToDevice, st));
+    k_iota<<<(r->capacity + 255) / 256, 256, 0, st>>>(r->q.freeStack, r->capacity);
+    CK(cudaGetLastError());
+    const int traceGrid = r->numSMs * 6, shadeGrid = r->numSMs * 4;
+    // bound on iterations: every path needs <= maxIter; waves of `capacity` paths
+    unsigned long long waves = c0.totalWork / r->capacity + 2;
+    unsigned long long maxIters = waves * (unsigned long long)(f.maxIter + 2) * 4ull + 64ull;
+    uint32_t iters = 0;
+    const uint32_t kChunk = 8;
+    const bool timing = (p->flags & WRK_FLAG_STAGE_TIMING) != 0;
+    // one event before and after each of the 8 launches of an iteration
+    if (timing && r->stageEv.size() < kChunk * 9) {
+        while (r->stageEv.size() < kChunk * 9) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            r->stageEv.push_back(e);
+        }
+    }
+    float stageMs[WRK_NUM_STAGES] = {0};
+    uint32_t stageN[WRK_NUM_STAGES] = {0};
+    CK(cudaEventRecord(r->evLoop0, st));
+    while (true) {
+        for (uint32_t k = 0; k < kChunk; ++k) {
+            cudaEvent_t* ev = timing ? &r->stageEv[k * 9] : nullptr;
+            if (timing) CK(cudaEventRecord(ev[0], st));
+            launch_control(r->q, st);
+            if (timing) CK(cudaEventRecord(ev[1], st));
+            launch_generate(r->q, r->soa, f, r->numSMs * 8, st);
+            if (timing) CK(cudaEventRecord(ev[2], st));
+            launch_trace_extension(s->view, r->q, r->soa, f, traceGrid, st);
+            if (timing) CK(cudaEventRecord(ev[3], st));
+            launch_trace_shadow(s->view, r->q, r->soa, traceGrid, st);
+            if (timing) CK(cudaEventRecord(ev[4], st));
+            for (uint32_t b = 0; b < kNumBuckets; ++b) {
+                launch_shade_bucket(b, s->view, r->q, r->soa, f, shadeGrid, st);
+                if (timing) CK(cudaEventRecord(ev[5 + b], st));
+            }
+        }
+        iters += kChunk;
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(r->hostCtr, r->q.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (timing) {
+            for (uint32_t k = 0; k < kChunk; ++k)
+                for (int j = 0; j < WRK_NUM_STAGES; ++j) {
+                    float ms = 0;
+                    CK(cudaEventElapsedTime(&ms, r->stageEv[k * 9 + j], r->stageEv[k * 9 + j + 1]));
+                    stageMs[j] += ms;
+                    stageN[j] += 1;
+                }
+        }
+        const Counters& h = *r->hostCtr;
+        uint32_t out = h.cur ^ 1u;
+        if (h.error) return fail(WRK_ERR_DEVICE, "device error flags 0x%x during render", h.error);
+        if (h.nextWork == h.totalWork && h.ext[out] == 0 && h.shd[out] == 0) break;
+        if (iters > maxIters) return fail(WRK_ERR_DEVICE, "render did not converge after %u iterations", iters);
+    }
+    CK(cudaEventRecord(r->evLoop1, st));
+    launch_resolve(f, p->flags & WRK_FLAG_RAW_GUIDES, d_rgb, d_alb, d_nrm, st);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(r->ev1, st));
+    CK(cudaEventSynchronize(r->ev1));
+    if (stats) {
+        const Counters& h = *r->hostCtr;
+        stats->paths = h.paths;
+        stats->extensionRays = h.extRays;
+        stats->shadowRays = h.shdRays;
+        stats->iterations = iters;
+        stats->deviceErrors = h.error;
+        cudaEventElapsedTime(&stats->gpuMs, r->evLoop0, r->evLoop1);
+        cudaEventElapsedTime(&stats->totalMs, r->ev0, r->ev1);
+        for (int j = 0; j < WRK_NUM_STAGES; ++j) {
+            stats->stageMs[j] = stageMs[j];
+            stats->stageLaunches[j] = stageN[j];
+        }
+    }
+    return WRK_OK;
+}
+
+static int check_render_args(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, const wrk_render_params* p) {
+    if (!r || !cam || !p) return fail(WRK_ERR_INVALID, "null renderer/camera/params");
+    int rc = check_scene(s);
+    if (rc) return rc;
+    if (s->device != r->device) return fail(WRK_ERR_INVALID, "scene and renderer on different devices");
+    if (p->width == 0 || p->height == 0 || p->spp == 0) return fail(WRK_ERR_INVALID, "empty render (w/h/spp = 0)");
+    if ((uint64_t)p->width * p->height > (1ull << 31)) return fail(WRK_ERR_INVALID, "image too large");
+    return WRK_OK;
+}
+
+int wrk_render_device(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, const wrk_render_params* p, float* d_rgb,
+                      float* d_alb, float* d_nrm, wrk_render_stats* stats) {
+    int rc = check_render_args(r, s, cam, p);
+    if (rc) return rc;
+    if (!d_rgb) return fail(WRK_ERR_INVALID, "null output");
+    return render_impl(r, s, cam, p, d_rgb, d_alb, d_nrm, stats);
+}
+
+int wrk_render(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, const wrk_render_params* p, float* rgb,
+               float* albedo, float* normal, wrk_render_stats* stats) {
+    int rc = check_render_args(r, s, cam, p);
+    if (rc) return rc;
+    if (!rgb) return fail(WRK_ERR_INVALID, "null output");
+    size_t np = (size_t)p->width * p->height;
+    if ((rc = r->outBufs.alloc(np * 9 * sizeof(float)))) return rc;
+    float* o = r->outBufs.as<float>();
+    if ((rc = render_impl(r, s, cam, p, o, albedo ? o + 3 * np : nullptr, normal ? o + 6 * np : nullptr, stats)))
+        return rc;
+    CK(cudaMemcpy(rgb, o, np * 3 * sizeof(float), cudaMemcpyDeviceToHost));
+    if (albedo) CK(cudaMemcpy(albedo, o + 3 * np, np * 3 * sizeof(float), cudaMemcpyDeviceToHost));
+    if (normal) CK(cudaMemcpy(normal, o + 6 * np, np * 3 * sizeof(float), cudaMemcpyDeviceToHost));
+    return WRK_OK;
+}
+
+// ---------------------------------------------------------------------------
+int wrk_trace_closest(wrk_scene* s, const float* rays, uint32_t n, float* t, uint32_t* prim) {
+    int rc = check_scene(s);
+    if (rc) return rc;
+    if (n && (!rays || !t || !prim)) return fail(WRK_ERR_INVALID, "null buffer");
+    CK(cudaMemset(s->dErr.p, 0, sizeof(uint32_t)));
+    launch_closest_query(s->view, rays, n, t, prim, s->dErr.as<uint32_t>(), 0);
+    CK(cudaGetLastError());
+    uint32_t e = 0;
+    CK(cudaMemcpy(&e, s->dErr.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (e) return fail(WRK_ERR_DEVICE, "trace error flags 0x%x", e);
+    return WRK_OK;
+}
+int wrk_trace_occluded(wrk_scene* s, const float* rays, uint32_t n, uint32_t* occ) {
+    int rc = check_scene(s);
+    if (rc) return rc;
+    if (n && (!rays || !occ)) return fail(WRK_ERR_INVALID, "null buffer");
+    CK(cudaMemset(s->dErr.p, 0, sizeof(uint32_t)));
+    launch_occluded_query(s->view, rays, n, occ, s->dErr.as<uint32_t>(), 0);
+    CK(cudaGetLastError());
+    uint32_t e = 0;
+    CK(cudaMemcpy(&e, s->dErr.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (e) return fail(WRK_ERR_DEVICE, "trace error flags 0x%x", e);
+    return WRK_OK;
+}
+int wrk_compact(const uint32_t* stage, const uint32_t* idxIn, uint32_t n, uint32_t* idxOut, uint32_t* count) {
+    if (!count || (n && (!stage || !idxIn || !idxOut))) return fail(WRK_ERR_INVALID, "null buffer");
+    int rc = compact_stable(stage, idxIn, n, idxOut, count, 0);
+    if (rc) return fail(rc, "compaction launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    CK(cudaDeviceSynchronize());
+    return WRK_OK;
+}
+int wrk_cdf_sample(const float* cdf, uint32_t ncdf, const float* u, uint32_t n, uint32_t* out) {
+    if (ncdf == 0) return fail(WRK_ERR_INVALID, "empty CDF");
+    launch_cdf(cdf, ncdf, u, n, out, 0);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    return WRK_OK;
+}
+int wrk_rng_batch(const uint32_t* seed, const uint32_t* dim, uint32_t n, uint32_t* hash, float* u) {
+    launch_rng(seed, dim, n, hash, u, 0);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    return WRK_OK;
+}
+int wrk_bsdf_batch(const float* in, uint32_t n, float* out) {
+    launch_bsdf(in, n, out, 0);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    return WRK_OK;
+}
+int wrk_texture_batch(wrk_scene* s, uint32_t id, const float* uv, uint32_t n, float* out) {
+    int rc = check_scene(s);
+    if (rc) return rc;
+    if (id == 0 || id > s->tex.size()) return fail(WRK_ERR_INVALID, "texture id %u out of range", id);
+    size_t off = 0;
+    for (uint32_t i = 0; i + 1 < id; ++i) off += (s->tex[i].size() + 15) & ~size_t(15);
+    launch_texture(s->dTexels.as<uint8_t>() + off, s->texW[id - 1], s->texH[id - 1], uv, n, out, 0);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    return WRK_OK;
+}
+int wrk_camera_rays(const wrk_camera* cam, uint32_t w, uint32_t h, const uint32_t* px, const uint32_t* sm, uint32_t n,
+                    uint32_t seed, float* out) {
+    if (!cam || w == 0 || h == 0) return fail(WRK_ERR_INVALID, "bad camera arguments");
+    Frame f{};
+    camera_frame(*cam, f);
+    f.width = w;
+    f.height = h;
+    f.seed = seed;
+    launch_camera_rays(f, px, sm, n, out, 0);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    return WRK_OK;
+}
+int wrk_tonemap_aces(const float* rgb, uint32_t npix, uint8_t* out) {
+    if (npix && (!rgb || !out)) return fail(WRK_ERR_INVALID, "null buffer");
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int vec = ((uintptr_t)rgb % 16 == 0 && (uintptr_t)out % 4 == 0) ? 1 : 0;
+    launch_tonemap(rgb, 3u * npix, out, sms * 8, vec, 0);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    return WRK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,519 @@
+// Wavefront path-tracing kernels: per-iteration control, camera-path generation,
+// material-bucketed shading, and the final resolve.  Together with the trace
+// kernels (trace.cu) they replace libWR's host loop and its raygen / closest-hit /
+// shade / compact programs (paths inside trianglestrip/OfflineRenderer):
+//   libWR/src/internal/renderer.cpp:190-313, libWR/kernels/trace.cu:17-319,
+//   libWR/kernels/shade.cu:24-85, libWR/kernels/materials/*.cuh,
+//   libWR/kernels/compact.cu:6-17.
+//
+// Paths live in SoA slots.  Each iteration:
+//   control   (1 thread)  swaps the extension/shadow queue buffers, clears the
+//                         material buckets, and pops free slots for new camera paths
+//   generate              camera rays for the next (sample, pixel) work items
+//   trace_extension       closest hit -> hit record + material bucket, or miss
+//   trace_shadow          any hit for pending NEE rays -> Lambert bucket (resume)
+//   shade<bucket> x4      closest-hit attributes, guides, emission, BSDF, RR;
+//                         appends to the next extension / shadow queue or frees
+// A path carries its own iteration count; after `maxIter` iterations (8 = the
+// reference host loop's cap) a live path is dropped unaccumulated, as libWR does.
+// RNG is keyed by (pixel, sample), so the image does not depend on queue order.
+#include "wrk_internal.h"
+#include "wrk_shading.cuh"
+
+namespace wrk {
+
+constexpr int kShadeBlock = 256;
+
+__device__ __forceinline__ void warp_append_r(uint32_t* q, uint32_t* counter, bool pred, uint32_t value,
+                                              uint32_t cap, uint32_t* err) {
+    uint32_t b = __ballot_sync(0xffffffffu, pred);
+    if (!b) return;
+    uint32_t lane = threadIdx.x & 31u;
+    uint32_t leader = __ffs(b) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(b));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    uint32_t pos = base + __popc(b & ((1u << lane) - 1u));
+    if (pred) {
+        if (pos < cap) q[pos] = value;
+        else atomicOr(err, kErrQueueOverflow);
+    }
+}
+
+__global__ void k_control(Queues q) {
+    Counters* c = q.ctr;
+    uint32_t cur = c->cur ^ 1u;
+    uint32_t out = cur ^ 1u;
+    c->cur = cur;
+    c->ext[out] = 0;
+    c->shd[out] = 0;
+    for (int b = 0; b < kNumBuckets; ++b) c->bucket[b] = 0;
+    unsigned long long remaining = c->totalWork - c->nextWork;
+    if (c->freeCount > q.capacity || c->ext[cur] > q.capacity) {
+        c->error |= kErrQueueOverflow;
+        c->freeCount = 0;
+    }
+    uint32_t g = (uint32_t)min((unsigned long long)c->freeCount, remaining);
+    g = min(g, q.capacity - c->ext[cur]);
+    c->genCount = g;
+    c->genFreeBase = c->freeCount - g;
+    c->freeCount -= g;
+    c->genWorkBase = c->nextWork;
+    c->nextWork += g;
+    c->genExtBase = c->ext[cur];
+    c->ext[cur] += g;
+    c->iteration += 1;
+}
+
+void launch_control(const Queues& q, cudaStream_t st) { k_control<<<1, 1, 0, st>>>(q); }
+
+// Camera ray for (pixel, sample): trace.cu:54-125.
+__global__ void __launch_bounds__(kShadeBlock) k_generate(Queues q, PathSoA p, Frame f) {
+    Counters* c = q.ctr;
+    const uint32_t g = c->genCount;
+    const uint32_t cur = c->cur;
+    const uint32_t fb = c->genFreeBase, eb = c->genExtBase;
+    const unsigned long long wb = c->genWorkBase;
+    uint32_t made = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g; i += gridDim.x * blockDim.x) {
+        uint32_t slot = q.freeStack[fb + i];
+        unsigned long long w = wb + i;
+        uint32_t sample = f.sampleOffset + (uint32_t)(w / f.perSample);
+        uint32_t j = (uint32_t)(w % f.perSample);
+        uint32_t x, y;
+        if (f.tilesX) {
+            uint32_t tile = j >> 5, lane = j & 31u;
+            x = (tile % f.tilesX) * 8u + (lane & 7u);
+            y = (tile / f.tilesX) * 4u + (lane >> 3);
+        } else {
+            x = j % f.width;
+            y = j / f.width;
+        }
+        uint32_t pixel = y * f.width + x;
+        uint32_t seed = path_seed(pixel, sample, f.seed);
+        uint32_t js = seed;
+        float r1 = lcg_randf(js);
+        float r2 = lcg_randf(js);
+        float nx = (2.0f * ((float)x + r1) / (float)f.width - 1.0f) * f.aspect;
+        float ny = 1.0f - 2.0f * ((float)y + r2) / (float)f.height;
+        float3 fwd = f3(f.fwd[0], f.fwd[1], f.fwd[2]), rt = f3(f.right[0], f.right[1], f.right[2]),
+               up = f3(f.up[0], f.up[1], f.up[2]), pos = f3(f.pos[0], f.pos[1], f.pos[2]);
+        float3 dir = normalize(add(add(fwd, mul(mul(rt, nx), f.tanHalf)), mul(mul(up, ny), f.tanHalf)));
+        float3 o = pos, d = dir;
+        if (f.lens > 0.0f && f.focal > 0.0f) {
+            float r3 = lcg_randf(js), r4 = lcg_randf(js);
+            float th = 2.0f * 3.14159265f * r3;
+            float rad = sqrtf(r4) * f.lens;
+            float ct = cosf(th), sn = sinf(th);
+            float3 off = f3(rt.x * rad * ct + up.x * rad * sn, rt.y * rad * ct + up.y * rad * sn,
+                            rt.z * rad * ct + up.z * rad * sn);
+            float3 fp = f3(pos.x + dir.x * f.focal, pos.y + dir.y * f.focal, pos.z + dir.z * f.focal);
+            o = f3(pos.x + off.x, pos.y + off.y, pos.z + off.z);
+            d = normalize(f3(fp.x - o.x, fp.y - o.y, fp.z - o.z));
+        }
+        p.ray_o[slot] = make_float4(o.x, o.y, o.z, 0.0001f);
+        p.ray_d[slot] = make_float4(d.x, d.y, d.z, 1e20f);
+        p.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+        p.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(pixel));
+        p.st[slot] = make_uint4(seed, 0u, 0u, kFlagFirstHit | kFlagPrevDelta);
+        q.ext[cur][eb + i] = slot;
+        ++made;
+    }
+    if (made) atomicAdd(&c->paths, (unsigned long long)made);
+}
+
+void launch_generate(const Queues& q, const PathSoA& p, const Frame& f, int grid, cudaStream_t st) {
+    k_generate<<<grid, kShadeBlock, 0, st>>>(q, p, f);
+}
+
+// ---------------------------------------------------------------------------
+// Closest-hit attributes (trace.cu:167-264): projected barycentrics, geometric and
+// interpolated shading normals (both flipped to face the ray), uv.
+struct HitAttr {
+    float3 pos, n, ng, e1, e2;
+    float u, v;
+    uint32_t mat, prim;
+};
+
+__device__ __forceinline__ float3 vtx3(const float* v, uint32_t i) {
+    return f3(__ldg(v + 3 * i), __ldg(v + 3 * i + 1), __ldg(v + 3 * i + 2));
+}
+
+__device__ __forceinline__ HitAttr hit_program(const DevScene& s, float3 o, float3 d, float t, uint32_t prim,
+                                               uint32_t mat) {
+    HitAttr h;
+    float3 hp = f3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
+    uint32_t i0 = __ldg(s.idx + 3 * prim), i1 = __ldg(s.idx + 3 * prim + 1), i2 = __ldg(s.idx + 3 * prim + 2);
+    float3 a = vtx3(s.vtx, i0), b = vtx3(s.vtx, i1), c = vtx3(s.vtx, i2);
+    float3 e1 = sub(b, a), e2 = sub(c, a);
+    float3 gn = normalize(cross(e1, e2));
+    float3 vp = sub(hp, a);
+    float d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(vp, e1), d21 = dot(vp, e2);
+    float den = d00 * d11 - d01 * d01;
+    float bv = (d11 * d20 - d01 * d21) / fmaxf(den, 1e-8f);
+    float bw = (d00 * d21 - d01 * d20) / fmaxf(den, 1e-8f);
+    float bu = 1.0f - bv - bw;
+    float3 sn = gn;
+    if (s.nrm) {
+        float3 n0 = vtx3(s.nrm, i0), n1 = vtx3(s.nrm, i1), n2 = vtx3(s.nrm, i2);
+        if (length(n0) > 1e-6f && length(n1) > 1e-6f && length(n2) > 1e-6f) {
+            sn = normalize(add(add(mul(bu, n0), mul(bv, n1)), mul(bw, n2)));
+            if (dot(sn, gn) < 0.0f) sn = neg(sn);
+        }
+    }
+    h.ng = dot(gn, d) > 0.0f ? neg(gn) : gn;
+    h.n = dot(sn, d) > 0.0f ? neg(sn) : sn;
+    h.pos = hp;
+    h.e1 = e1;
+    h.e2 = e2;
+    h.mat = mat;
+    h.prim = prim;
+    if (s.uv) {
+        h.u = bu * __ldg(s.uv + 2 * i0) + bv * __ldg(s.uv + 2 * i1) + bw * __ldg(s.uv + 2 * i2);
+        h.v = bu * __ldg(s.uv + 2 * i0 + 1) + bv * __ldg(s.uv + 2 * i1 + 1) + bw * __ldg(s.uv + 2 * i2 + 1);
+    } else {
+        h.u = h.v = 0.0f;
+    }
+    return h;
+}
+
+// getMaterialAlbedo (materials.cuh:25-29): 1-based texture id, else the constant.
+__device__ __forceinline__ float3 albedo_of(const DevScene& s, const wrk_material& m, float u, float v) {
+    if (m.albedoTextureId != 0 && m.albedoTextureId <= s.numTex) {
+        TexInfo ti = s.tex[m.albedoTextureId - 1];
+        if (ti.w == 0) return f3(1, 1, 1);
+        float4 c = tex_fetch(s.texels + ti.offset, ti.w, ti.h, u, v);
+        return f3(c.x, c.y, c.z);
+    }
+    return f3(m.albedo[0], m.albedo[1], m.albedo[2]);
+}
+
+// getEffectiveNormal (normal_map.cuh:40-60).
+__device__ __forceinline__ float3 normal_mapped(const DevScene& s, const wrk_material& m, const HitAttr& h) {
+    if (m.normalTextureId > 0 && m.normalTextureId <= s.numTex) {
+        TexInfo ti = s.tex[m.normalTextureId - 1];
+        float4 c = ti.w ? tex_fetch(s.texels + ti.offset, ti.w, ti.h, h.u, h.v) : make_float4(0.5f, 0.5f, 1.0f, 1.0f);
+        float3 tg, bt;
+        frame(h.n, tg, bt);
+        float3 q = f3(c.x * 2.0f - 1.0f, c.y * 2.0f - 1.0f, c.z * 2.0f - 1.0f);
+        return normalize(f3(tg.x * q.x + bt.x * q.y + h.n.x * q.z, tg.y * q.x + bt.y * q.y + h.n.y * q.z,
+                            tg.z * q.x + bt.z * q.y + h.n.z * q.z));
+    }
+    return h.n;
+}
+
+enum : int { kOutNone = 0, kOutExt = 1, kOutShadow = 2, kOutFree = 3 };
+
+struct PathRegs {
+    float3 o, d, thr, rad;
+    float prevPdf;
+    uint32_t pixel, seed, dim, depth, iter, flags;
+};
+
+__device__ __forceinline__ void accumulate(const Frame& f, const PathRegs& r) {
+    float3 L = clamp_fireflies(r.rad, f.fireflyClamp);
+    atomicAdd(f.accum + r.pixel, make_float4(L.x, L.y, L.z, 0.0f));
+}
+
+// setupNextBounce (material_common.cuh:55-71); returns the outcome.
+__device__ __forceinline__ int next_bounce(const Frame& f, PathRegs& r, const HitAttr& h, float3 nd) {
+    r.d = nd;
+    r.o = offset_origin(h.pos, h.n, nd);
+    r.depth += 1;
+    if (r.depth >= f.maxBounces) {
+        accumulate(f, r);
+        return kOutFree;
+    }
+    return kOutExt;
+}
+
+__device__ __forceinline__ bool rr(const Frame& f, PathRegs& r, bool delta) {
+    float3 nt;
+    float xi = rnd_dim(r.seed, r.dim++);
+    if (!russian_roulette(r.thr, r.depth, f.rrStart, xi, nt, delta)) {
+        accumulate(f, r);
+        return false;
+    }
+    r.thr = nt;
+    return true;
+}
+
+// NEE light sample (lambertian.cuh:17-63, ggx_material.cuh:51-95): picks a light
+// through the power CDF, samples a point on it; returns false if not facing.
+struct LightSample {
+    float3 toLight, le;
+    float dist, d2, lpdf, cosTheta;
+};
+__device__ __forceinline__ bool sample_light(const DevScene& s, PathRegs& r, const HitAttr& h, LightSample& ls) {
+    float lu = rnd_dim(r.seed, r.dim++);
+    uint32_t li = cdf_lower_bound(lu, s.cdf, s.numEmissive);
+    uint32_t tri = __ldg(s.emissive + li);
+    uint32_t i0 = __ldg(s.idx + 3 * tri), i1 = __ldg(s.idx + 3 * tri + 1), i2 = __ldg(s.idx + 3 * tri + 2);
+    float3 a = vtx3(s.vtx, i0), b = vtx3(s.vtx, i1), c = vtx3(s.vtx, i2);
+    // two uniforms in one call: the earlier dimension is the first argument
+    float u1 = rnd_dim(r.seed, r.dim++);
+    float u2 = rnd_dim(r.seed, r.dim++);
+    float3 ln;
+    float la;
+    float3 lp = sample_triangle(u1, u2, a, b, c, ln, la);
+    float3 tl = f3(lp.x - h.pos.x, lp.y - h.pos.y, lp.z - h.pos.z);
+    float d2 = dot(tl, tl);
+    float dist = sqrtf(d2);
+    tl = f3(tl.x / dist, tl.y / dist, tl.z / dist);
+    float ct = dot(h.n, tl);
+    float cl = -dot(ln, tl);
+    if (!(ct > 0.0f && cl > 0.0f)) return false;
+    const wrk_material& lm = s.mats[__ldg(s.triMat + tri)];
+    float pa = 1.0f / ((float)s.numEmissive * la);
+    ls.lpdf = pa * d2 / fmaxf(cl, 1e-8f);
+    ls.toLight = tl;
+    ls.dist = dist;
+    ls.d2 = d2;
+    ls.cosTheta = ct;
+    ls.le = f3(lm.emission[0], lm.emission[1], lm.emission[2]);
+    return true;
+}
+
+template <uint32_t kBucket>
+__device__ __forceinline__ int shade_one(const DevScene& s, const PathSoA& p, const Frame& f, uint32_t slot) {
+    float4 o4 = p.ray_o[slot], d4 = p.ray_d[slot], h4 = p.hit[slot], t4 = p.thr[slot], r4 = p.rad[slot];
+    uint4 st = p.st[slot];
+    PathRegs r;
+    r.o = f3(o4.x, o4.y, o4.z);
+    r.d = f3(d4.x, d4.y, d4.z);
+    r.thr = f3(t4.x, t4.y, t4.z);
+    r.prevPdf = t4.w;
+    r.rad = f3(r4.x, r4.y, r4.z);
+    r.pixel = __float_as_uint(r4.w);
+    r.seed = st.x;
+    r.dim = st.y;
+    r.depth = st.z & 0xffffu;
+    r.iter = st.z >> 16;
+    r.flags = st.w;
+    uint32_t mat = __float_as_uint(h4.z);
+    uint32_t prim = __float_as_uint(h4.y);
+    if (prim >= s.numTris) {
+        atomicOr(f.err, kErrBadIndex);
+        return kOutFree;
+    }
+    HitAttr h = hit_program(s, r.o, r.d, h4.x, prim, mat);
+    const bool matOk = mat < s.numMats;
+    // first-hit guides (trace.cu:267-286)
+    if (r.flags & kFlagFirstHit) {
+        if (matOk) {
+            float3 al = albedo_of(s, s.mats[mat], h.u, h.v);
+            if (f.albedo) atomicAdd(f.albedo + r.pixel, make_float4(al.x, al.y, al.z, 0.0f));
+            if (f.normal) atomicAdd(f.normal + r.pixel, make_float4(h.ng.x, h.ng.y, h.ng.z, 0.0f));
+        }
+        r.flags &= ~kFlagFirstHit;
+    }
+    int out = kOutNone;
+    if (kBucket == kBucketOther) {
+        if (!matOk) return kOutFree;  // shade.cu:35-38: terminated without accumulation
+        const wrk_material m = s.mats[mat];
+        if (m.type == kEmissive) {  // emission with MIS (trace.cu:288-316)
+            float w = 1.0f;
+            if (f.useNEE && r.depth > 0 && !(r.flags & kFlagPrevDelta) && s.numEmissive > 0) {
+                float area = 0.5f * length(cross(h.e1, h.e2));
+                float d2 = h4.x * h4.x;
+                float cl = fabsf(dot(h.ng, r.d));
+                float pa = 1.0f / ((float)s.numEmissive * area);
+                float lpdf = pa * d2 / fmaxf(cl, 1e-8f);
+                w = power_heuristic(r.prevPdf, lpdf);
+            }
+            float3 em = f3(m.emission[0], m.emission[1], m.emission[2]);
+            r.rad = add(r.rad, mul(mul(r.thr, em), w));
+        }
+        accumulate(f, r);  // shadeEmissive / default branch: terminateRay
+        return kOutFree;
+    }
+    const wrk_material m = s.mats[mat];
+    if (m.normalTextureId > 0) h.n = normal_mapped(s, m, h);
+    if (kBucket == kBucketLambert) {
+        if (f.useNEE && s.numEmissive > 0 && !(r.flags & kFlagNeeDone)) {
+            LightSample ls;
+            if (sample_light(s, r, h, ls)) {
+                float bpdf = cosine_pdf(ls.cosTheta);
+                float w = power_heuristic(ls.lpdf, bpdf);
+                float3 al = albedo_of(s, m, h.u, h.v);
+                float3 fb = f3(al.x / kPi * ls.cosTheta, al.y / kPi * ls.cosTheta, al.z / kPi * ls.cosTheta);
+                float3 con = f3(r.thr.x * fb.x * ls.le.x * w / ls.lpdf, r.thr.y * fb.y * ls.le.y * w / ls.lpdf,
+                                r.thr.z * fb.z * ls.le.z * w / ls.lpdf);
+                if (finite3(con) && con.x >= 0.0f && con.y >= 0.0f && con.z >= 0.0f) {
+                    float3 so = offset_origin(h.pos, h.n, ls.toLight);
+                    p.sh_o[slot] = make_float4(so.x, so.y, so.z, 1e-5f);
+                    p.sh_d[slot] = make_float4(ls.toLight.x, ls.toLight.y, ls.toLight.z, ls.dist - 1e-5f);
+                    p.sh_c[slot] = make_float4(con.x, con.y, con.z, 0.0f);
+                    r.flags |= kFlagNeeDone;
+                    out = kOutShadow;
+                }
+            }
+        }
+        if (out == kOutNone) {
+            r.flags &= ~kFlagNeeDone;
+            float3 tg, bt;
+            frame(h.n, tg, bt);
+            float u1 = rnd_dim(r.seed, r.dim++);
+            float u2 = rnd_dim(r.seed, r.dim++);
+            float pdf;
+            float3 loc = cosine_hemisphere(u1, u2, pdf);
+            float3 wd = to_world(loc, h.n, tg, bt);
+            float3 al = albedo_of(s, m, h.u, h.v);
+            r.thr = mul(r.thr, al);
+            r.prevPdf = pdf;
+            r.flags &= ~kFlagPrevDelta;
+            if (!rr(f, r, false)) return kOutFree;
+            out = next_bounce(f, r, h, wd);
+        }
+    } else if (kBucket == kBucketDielectric) {
+        float3 wo = neg(r.d);
+        float ci = dot(wo, h.n);
+        float ei = 1.0f, et = m.ior;
+        float3 n = h.n;
+        if (ci < 0.0f) { ci = -ci; n = neg(n); ei = m.ior; et = 1.0f; }
+        float F = fresnel_dielectric(ci, ei, et);
+        float xi = rnd_dim(r.seed, r.dim++);
+        float3 al = albedo_of(s, m, h.u, h.v);
+        if (xi < F) {
+            r.d = sub(r.d, mul(n, 2.0f * dot(r.d, n)));
+            r.thr = f3(r.thr.x * al.x, r.thr.y * al.y, r.thr.z * al.z);
+        } else {
+            float eta = ei / et;
+            float s2 = eta * eta * (1.0f - ci * ci);
+            if (s2 >= 1.0f) {
+                r.d = sub(r.d, mul(n, 2.0f * dot(r.d, n)));
+                r.thr = f3(r.thr.x * al.x, r.thr.y * al.y, r.thr.z * al.z);
+            } else {
+                float ct = sqrtf(fmaxf(0.0f, 1.0f - s2));
+                float3 rf = add(mul(eta, r.d), mul(n, eta * ci - ct));
+                r.d = rf;
+                r.thr = f3(r.thr.x * al.x, r.thr.y * al.y, r.thr.z * al.z);
+                float k = shading_correction(rf, h.n, h.ng);
+                r.thr = f3(r.thr.x * k, r.thr.y * k, r.thr.z * k);
+            }
+        }
+        r.flags |= kFlagPrevDelta;
+        if (!rr(f, r, true)) return kOutFree;
+        out = next_bounce(f, r, h, r.d);
+    } else {  // GGX reflection
+        float3 wo = neg(r.d);
+        float3 alb = f3(m.albedo[0], m.albedo[1], m.albedo[2]);
+        if (f.useNEE && s.numEmissive > 0) {
+            LightSample ls;
+            if (sample_light(s, r, h, ls)) {
+                float3 fb = ggx_eval(wo, ls.toLight, h.n, alb, m.roughness, m.metallic, m.ior);
+                float bpdf = ggx_pdf(wo, ls.toLight, h.n, m.roughness);
+                float w = power_heuristic(ls.lpdf, bpdf);
+                float3 con = f3(r.thr.x * fb.x * ls.le.x * ls.cosTheta * w / ls.lpdf,
+                                r.thr.y * fb.y * ls.le.y * ls.cosTheta * w / ls.lpdf,
+                                r.thr.z * fb.z * ls.le.z * ls.cosTheta * w / ls.lpdf);
+                if (finite3(con) && con.x >= 0.0f && con.y >= 0.0f && con.z >= 0.0f)
+                    r.rad = f3(r.rad.x + con.x, r.rad.y + con.y, r.rad.z + con.z);
+            }
+        }
+        float3 tg, bt;
+        frame(h.n, tg, bt);
+        float3 wi = f3(0, 0, 0);
+        float pdf = 0.0f;
+        float u0 = rnd_dim(r.seed, r.dim++);
+        float u1 = rnd_dim(r.seed, r.dim++);
+        ggx_sample(wo, h.n, tg, bt, m.roughness, u0, u1, wi, pdf);
+        float ct = dot(h.n, wi);
+        if (pdf < 1e-5f || ct <= 0.0f) {
+            accumulate(f, r);
+            return kOutFree;
+        }
+        float3 fb = ggx_eval(wo, wi, h.n, alb, m.roughness, m.metallic, m.ior);
+        if (!finite3(fb)) {
+            accumulate(f, r);
+            return kOutFree;
+        }
+        r.thr = f3(r.thr.x * fb.x * ct / pdf, r.thr.y * fb.y * ct / pdf, r.thr.z * fb.z * ct / pdf);
+        r.prevPdf = pdf;
+        r.flags &= ~kFlagPrevDelta;
+        if (!rr(f, r, false)) return kOutFree;
+        out = next_bounce(f, r, h, wi);
+    }
+    // continuing path: iteration cap (renderer.cpp:213) then write back
+    if (out == kOutExt || out == kOutShadow) {
+        if (r.iter + 1u >= f.maxIter) return kOutFree;  // dropped, nothing accumulated
+        r.iter += 1u;
+        if (out == kOutExt) {
+            p.ray_o[slot] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
+            p.ray_d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 1e20f);
+        }
+        p.thr[slot] = make_float4(r.thr.x, r.thr.y, r.thr.z, r.prevPdf);
+        p.rad[slot] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
+        p.st[slot] = make_uint4(r.seed, r.dim, (r.depth & 0xffffu) | (r.iter << 16), r.flags);
+    }
+    return out;
+}
+
+template <uint32_t kBucket>
+__global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, Queues q, PathSoA p, Frame f) {
+    Counters* c = q.ctr;
+    const uint32_t cur = c->cur, nxt = cur ^ 1u;
+    const uint32_t n = min(c->bucket[kBucket], q.capacity);
+    const uint32_t* in = q.bucket[kBucket];
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        uint32_t i = base + threadIdx.x;
+        uint32_t slot = i < n ? in[i] : kInvalidSlot;
+        if (slot != kInvalidSlot && slot >= q.capacity) {
+            atomicOr(&c->error, kErrBadIndex);
+            slot = kInvalidSlot;
+        }
+        int out = slot != kInvalidSlot ? shade_one<kBucket>(s, p, f, slot) : kOutNone;
+        warp_append_r(q.ext[nxt], &c->ext[nxt], out == kOutExt, slot, q.capacity, &c->error);
+        warp_append_r(q.shd[nxt], &c->shd[nxt], out == kOutShadow, slot, q.capacity, &c->error);
+        warp_append_r(q.freeStack, &c->freeCount, out == kOutFree, slot, q.capacity, &c->error);
+    }
+}
+
+void launch_shade_bucket(uint32_t b, const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid,
+                         cudaStream_t st) {
+    switch (b) {
+        case kBucketLambert: k_shade<kBucketLambert><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
+        case kBucketDielectric: k_shade<kBucketDielectric><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
+        case kBucketGGX: k_shade<kBucketGGX><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
+        default: k_shade<kBucketOther><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
+    }
+}
+
+void launch_shade(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid, cudaStream_t st) {
+    k_shade<kBucketLambert><<<grid, kShadeBlock, 0, st>>>(s, q, p, f);
+    k_shade<kBucketDielectric><<<grid, kShadeBlock, 0, st>>>(s, q, p, f);
+    k_shade<kBucketGGX><<<grid, kShadeBlock, 0, st>>>(s, q, p, f);
+    k_shade<kBucketOther><<<grid, kShadeBlock, 0, st>>>(s, q, p, f);
+}
+
+// rgb = sum * (1/spp) as renderer.cpp:308-313; guides averaged unless raw.
+__global__ void k_resolve(Frame f, uint32_t raw, float* rgb, float* albedo, float* normal) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t n = f.width * f.height;
+    if (i >= n) return;
+    float inv = 1.0f / (float)f.spp;
+    float4 a = f.accum[i];
+    rgb[3 * i] = a.x * inv;
+    rgb[3 * i + 1] = a.y * inv;
+    rgb[3 * i + 2] = a.z * inv;
+    float g = raw ? 1.0f : inv;
+    if (albedo) {
+        float4 b = f.albedo[i];
+        albedo[3 * i] = b.x * g;
+        albedo[3 * i + 1] = b.y * g;
+        albedo[3 * i + 2] = b.z * g;
+    }
+    if (normal) {
+        float4 b = f.normal[i];
+        normal[3 * i] = b.x * g;
+        normal[3 * i + 1] = b.y * g;
+        normal[3 * i + 2] = b.z * g;
+    }
+}
+
+void launch_resolve(const Frame& f, uint32_t raw, float* rgb, float* albedo, float* normal, cudaStream_t st) {
+    uint32_t n = f.width * f.height;
+    k_resolve<<<(n + 255) / 256, 256, 0, st>>>(f, raw, rgb, albedo, normal);
+}
+
+}  // namespace wrk

@@ -1,0 +1,335 @@
+// Ray traversal of the 8-wide compressed BVH: closest hit (extension rays) and
+// any hit (shadow rays).  Replaces optixTrace with __closesthit__trace /
+// __miss__trace (libWR/kernels/trace.cu:17-153,321-323 in trianglestrip/OfflineRenderer);
+// there are no RT cores on B200, so traversal is SIMT integer/FP32 work.
+//
+// Per node: five 16-byte loads (__ldg, read-only path), eight quantized slab tests
+// decoded with one FMA per plane.  Internal-child hits go into an 8-bit mask
+// permuted by the ray octant so the lowest set bit is the child nearest the ray's
+// entry corner; leaf-child hits set bits of a triangle mask.  Pending node groups
+// (child base + remaining hit bits + internal mask) go on a short stack held in
+// shared memory, spilling to a bounded local array; overflow raises an error bit
+// and ends the ray instead of corrupting memory.
+//
+// The triangle test is Moller-Trumbore written with _rn intrinsics so the FP32
+// result is the same sequence of correctly rounded operations as the CPU oracle's.
+#include "wrk_internal.h"
+#include "wrk_shading.cuh"
+
+namespace wrk {
+
+constexpr int kTraceBlock = 128;
+constexpr int kStackSmem = 12;
+constexpr int kStackLocal = 36;
+constexpr uint32_t kMaxVisits = 1u << 16;
+
+struct Ray {
+    float ox, oy, oz, dx, dy, dz, tmin, tmax;
+};
+
+__device__ __forceinline__ bool mt_rn(const Ray& r, float4 a, float4 b, float4 c, float& t) {
+    // pvec = d x e2, det = e1 . pvec, tvec = o - v0, u = tvec.pvec / det ...
+    float px = __fsub_rn(__fmul_rn(r.dy, c.z), __fmul_rn(r.dz, c.y));
+    float py = __fsub_rn(__fmul_rn(r.dz, c.x), __fmul_rn(r.dx, c.z));
+    float pz = __fsub_rn(__fmul_rn(r.dx, c.y), __fmul_rn(r.dy, c.x));
+    float det = __fadd_rn(__fadd_rn(__fmul_rn(b.x, px), __fmul_rn(b.y, py)), __fmul_rn(b.z, pz));
+    if (det == 0.0f) return false;
+    float inv = __frcp_rn(det);
+    float sx = __fsub_rn(r.ox, a.x), sy = __fsub_rn(r.oy, a.y), sz = __fsub_rn(r.oz, a.z);
+    float u = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(sx, px), __fmul_rn(sy, py)), __fmul_rn(sz, pz)), inv);
+    if (!(u >= 0.0f && u <= 1.0f)) return false;
+    float qx = __fsub_rn(__fmul_rn(sy, b.z), __fmul_rn(sz, b.y));
+    float qy = __fsub_rn(__fmul_rn(sz, b.x), __fmul_rn(sx, b.z));
+    float qz = __fsub_rn(__fmul_rn(sx, b.y), __fmul_rn(sy, b.x));
+    float v = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(r.dx, qx), __fmul_rn(r.dy, qy)), __fmul_rn(r.dz, qz)), inv);
+    if (!(v >= 0.0f && __fadd_rn(u, v) <= 1.0f)) return false;
+    t = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(c.x, qx), __fmul_rn(c.y, qy)), __fmul_rn(c.z, qz)), inv);
+    return true;
+}
+
+__device__ __forceinline__ uint32_t byte_of(uint32_t w, int k) { return (w >> (8 * k)) & 0xffu; }
+
+// Intersects the 8 children of a node; returns internal hits (permuted by octant)
+// and the triangle mask relative to triBase.
+__device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, uint32_t idx, const Ray& r,
+                                               float ix, float iy, float iz, uint32_t oct_inv, float tfar_max,
+                                               uint32_t& childBase, uint32_t& triBase, uint32_t& hits,
+                                               uint32_t& imask, uint32_t& tmask) {
+    const uint4* n = nodes + 5 * (size_t)idx;
+    uint4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2), n3 = __ldg(n + 3), n4 = __ldg(n + 4);
+    float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
+    float sx = __uint_as_float((n0.w & 0xffu) << 23) * ix;
+    float sy = __uint_as_float(((n0.w >> 8) & 0xffu) << 23) * iy;
+    float sz = __uint_as_float(((n0.w >> 16) & 0xffu) << 23) * iz;
+    float ax = (px - r.ox) * ix, ay = (py - r.oy) * iy, az = (pz - r.oz) * iz;
+    imask = n0.w >> 24;
+    childBase = n1.x;
+    triBase = n1.y;
+    hits = 0;
+    tmask = 0;
+    // near/far plane words per axis: dir >= 0 -> near = lo, far = hi
+    uint32_t xn0 = ix >= 0.0f ? n2.x : n3.z, xn1 = ix >= 0.0f ? n2.y : n3.w;
+    uint32_t xf0 = ix >= 0.0f ? n3.z : n2.x, xf1 = ix >= 0.0f ? n3.w : n2.y;
+    uint32_t yn0 = iy >= 0.0f ? n2.z : n4.x, yn1 = iy >= 0.0f ? n2.w : n4.y;
+    uint32_t yf0 = iy >= 0.0f ? n4.x : n2.z, yf1 = iy >= 0.0f ? n4.y : n2.w;
+    uint32_t zn0 = iz >= 0.0f ? n3.x : n4.z, zn1 = iz >= 0.0f ? n3.y : n4.w;
+    uint32_t zf0 = iz >= 0.0f ? n4.z : n3.x, zf1 = iz >= 0.0f ? n4.w : n3.y;
+    const float tfar_lim = tfar_max * 1.00000024f;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        int k = s & 3;
+        uint32_t xn = s < 4 ? xn0 : xn1, xf = s < 4 ? xf0 : xf1;
+        uint32_t yn = s < 4 ? yn0 : yn1, yf = s < 4 ? yf0 : yf1;
+        uint32_t zn = s < 4 ? zn0 : zn1, zf = s < 4 ? zf0 : zf1;
+        float t0x = fmaf((float)byte_of(xn, k), sx, ax);
+        float t1x = fmaf((float)byte_of(xf, k), sx, ax);
+        float t0y = fmaf((float)byte_of(yn, k), sy, ay);
+        float t1y = fmaf((float)byte_of(yf, k), sy, ay);
+        float t0z = fmaf((float)byte_of(zn, k), sz, az);
+        float t1z = fmaf((float)byte_of(zf, k), sz, az);
+        float tn = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, r.tmin));
+        float tf = fminf(fminf(t1x, t1y), fminf(t1z, tfar_lim));
+        if (tn <= tf * 1.00000024f) {
+            uint32_t meta = byte_of(s < 4 ? n1.z : n1.w, k);
+            if ((imask >> s) & 1u) {
+                hits |= 1u << (s ^ oct_inv);
+            } else {
+                uint32_t cnt = (meta >> 5) + 1u, off = meta & 31u;
+                tmask |= ((1u << cnt) - 1u) << off;
+            }
+        }
+    }
+}
+
+// Closest hit with ties broken toward the lower primitive index.  Returns false
+// on miss.  *err gets kErrStackOverflow if the stack limit is reached.
+template <bool kAnyHit>
+__device__ __forceinline__ bool traverse(const DevScene& s, const Ray& r, float& tBest, uint32_t& pBest,
+                                         uint32_t& mBest, uint2* sstack, uint32_t* errFlag) {
+    float ix = 1.0f / r.dx, iy = 1.0f / r.dy, iz = 1.0f / r.dz;
+    uint32_t oct = (r.dx < 0.0f ? 1u : 0u) | (r.dy < 0.0f ? 2u : 0u) | (r.dz < 0.0f ? 4u : 0u);
+    uint32_t oct_inv = oct ^ 7u;  // slot of the child nearest the entry corner -> bit 0
+    tBest = r.tmax;
+    pBest = kNoHit;
+    mBest = 0;
+    uint2 lstack[kStackLocal];
+    int sp = 0;
+    // node group: (base, hits, imask); the root is a one-child group
+    uint32_t gBase = 0, gHits = 1u << (0u ^ oct_inv), gImask = 1u;
+    uint32_t tBase = 0, tMask = 0;
+    const int tid = threadIdx.x;
+    uint32_t visits = 0;
+    while (true) {
+        if (++visits > kMaxVisits) {  // a malformed tree must not spin forever
+            atomicOr(errFlag, kErrBadIndex);
+            return pBest != kNoHit;
+        }
+        if (gHits) {
+            uint32_t pos = __ffs(gHits) - 1;
+            gHits &= gHits - 1;
+            uint32_t slot = pos ^ oct_inv;
+            uint32_t child = gBase + __popc(gImask & ((1u << slot) - 1u));
+            if (gHits) {
+                uint2 e = make_uint2(gBase, gHits | (gImask << 8));
+                if (sp < kStackSmem) sstack[sp * kTraceBlock + tid] = e;
+                else if (sp < kStackSmem + kStackLocal) lstack[sp - kStackSmem] = e;
+                else { atomicOr(errFlag, kErrStackOverflow); return pBest != kNoHit; }
+                ++sp;
+            }
+            if (child >= s.numNodes) {
+                atomicOr(errFlag, kErrBadIndex);
+                return pBest != kNoHit;
+            }
+            intersect_node(s.nodes, child, r, ix, iy, iz, oct_inv, tBest, gBase, tBase, gHits, gImask, tMask);
+            if (tMask && tBase + (31u - __clz(tMask)) >= s.numTris) {
+                atomicOr(errFlag, kErrBadIndex);
+                return pBest != kNoHit;
+            }
+        }
+        while (tMask) {
+            uint32_t j = __ffs(tMask) - 1;
+            tMask &= tMask - 1;
+            const float4* tp = s.tris + 3 * (size_t)(tBase + j);
+            float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+            float t;
+            if (mt_rn(r, a, b, c, t) && t >= r.tmin && t <= r.tmax) {
+                uint32_t prim = __float_as_uint(a.w);
+                if (kAnyHit) {
+                    tBest = t;
+                    pBest = prim;
+                    return true;
+                }
+                if (t < tBest || (t == tBest && prim < pBest)) {
+                    tBest = t;
+                    pBest = prim;
+                    mBest = __float_as_uint(b.w);
+                }
+            }
+        }
+        if (!gHits) {
+            if (sp == 0) break;
+            --sp;
+            uint2 e = sp < kStackSmem ? sstack[sp * kTraceBlock + tid] : lstack[sp - kStackSmem];
+            gBase = e.x;
+            gHits = e.y & 0xffu;
+            gImask = e.y >> 8;
+        }
+    }
+    return pBest != kNoHit;
+}
+
+__device__ __forceinline__ Ray load_ray8(const float* p) {
+    float4 a = *reinterpret_cast<const float4*>(p);
+    float4 b = *reinterpret_cast<const float4*>(p + 4);
+    return Ray{a.x, a.y, a.z, b.x, b.y, b.z, a.w, b.w};
+}
+
+__global__ void __launch_bounds__(kTraceBlock) k_closest_query(DevScene s, const float* __restrict__ rays, uint32_t n,
+                                                               float* tOut, uint32_t* pOut, uint32_t* err) {
+    __shared__ uint2 sstack[kStackSmem * kTraceBlock];
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Ray r = load_ray8(rays + 8 * (size_t)i);
+    float t;
+    uint32_t p, m;
+    bool hit = traverse<false>(s, r, t, p, m, sstack, err);
+    tOut[i] = hit ? t : __int_as_float(0x7f800000);
+    pOut[i] = hit ? p : kNoHit;
+}
+
+__global__ void __launch_bounds__(kTraceBlock) k_occluded_query(DevScene s, const float* __restrict__ rays,
+                                                                uint32_t n, uint32_t* out, uint32_t* err) {
+    __shared__ uint2 sstack[kStackSmem * kTraceBlock];
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Ray r = load_ray8(rays + 8 * (size_t)i);
+    float t;
+    uint32_t p, m;
+    out[i] = traverse<true>(s, r, t, p, m, sstack, err) ? 1u : 0u;
+}
+
+void launch_closest_query(const DevScene& s, const float* rays, uint32_t n, float* t, uint32_t* prim, uint32_t* err,
+                          cudaStream_t st) {
+    if (!n) return;
+    k_closest_query<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, st>>>(s, rays, n, t, prim, err);
+}
+void launch_occluded_query(const DevScene& s, const float* rays, uint32_t n, uint32_t* occ, uint32_t* err,
+                           cudaStream_t st) {
+    if (!n) return;
+    k_occluded_query<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, st>>>(s, rays, n, occ, err);
+}
+
+// ---------------------------------------------------------------------------
+// Wavefront trace kernels.  Queue appends are warp-aggregated: one ballot per
+// destination queue, one atomicAdd by the lowest active lane, positions by popc.
+__device__ __forceinline__ void warp_append(uint32_t* q, uint32_t* counter, bool pred, uint32_t value,
+                                            uint32_t cap, uint32_t* err) {
+    uint32_t b = __ballot_sync(0xffffffffu, pred);
+    if (!b) return;
+    uint32_t lane = threadIdx.x & 31u;
+    uint32_t leader = __ffs(b) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(b));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    uint32_t pos = base + __popc(b & ((1u << lane) - 1u));
+    if (pred) {
+        if (pos < cap) q[pos] = value;
+        else atomicOr(err, kErrQueueOverflow);
+    }
+}
+__device__ __forceinline__ void warp_count64(unsigned long long* counter, bool pred) {
+    uint32_t b = __ballot_sync(0xffffffffu, pred);
+    if (b && (threadIdx.x & 31u) == (uint32_t)(__ffs(b) - 1)) atomicAdd(counter, (unsigned long long)__popc(b));
+}
+
+__device__ __forceinline__ uint32_t bucket_of(uint32_t type) {
+    switch (type) {
+        case kLambert: return kBucketLambert;
+        case kGlass:
+        case kGGXT: return kBucketDielectric;
+        case kGGX: return kBucketGGX;
+        default: return kBucketOther;
+    }
+}
+
+__global__ void __launch_bounds__(kTraceBlock) k_trace_extension(DevScene s, Queues q, PathSoA p, Frame f) {
+    __shared__ uint2 sstack[kStackSmem * kTraceBlock];
+    Counters* c = q.ctr;
+    const uint32_t cur = c->cur;
+    const uint32_t n = min(c->ext[cur], q.capacity);
+    const uint32_t* in = q.ext[cur];
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        uint32_t i = base + threadIdx.x;
+        uint32_t slot = i < n ? in[i] : kInvalidSlot;
+        if (slot != kInvalidSlot && slot >= q.capacity) {
+            atomicOr(&c->error, kErrBadIndex);
+            slot = kInvalidSlot;
+        }
+        bool valid = slot != kInvalidSlot;
+        bool hit = false, miss = false;
+        uint32_t bucket = kNumBuckets;
+        if (valid) {
+            float4 o = p.ray_o[slot], d = p.ray_d[slot];
+            Ray r{o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w};
+            float t;
+            uint32_t prim, mat;
+            hit = traverse<false>(s, r, t, prim, mat, sstack, &c->error);
+            if (hit) {
+                p.hit[slot] = make_float4(t, __uint_as_float(prim), __uint_as_float(mat), 0.0f);
+                bucket = mat < s.numMats ? bucket_of(s.mats[mat].type) : kBucketOther;
+            } else {
+                // __miss__trace + raygen miss branch (trace.cu:143-148): add T*env, accumulate, terminate
+                miss = true;
+                float4 th = p.thr[slot], rd = p.rad[slot];
+                float3 L = make_float3(rd.x + th.x * s.env[0], rd.y + th.y * s.env[1], rd.z + th.z * s.env[2]);
+                L = clamp_fireflies(L, f.fireflyClamp);
+                atomicAdd(f.accum + __float_as_uint(rd.w), make_float4(L.x, L.y, L.z, 0.0f));
+            }
+        }
+        warp_count64(&c->extRays, valid);
+#pragma unroll
+        for (uint32_t b = 0; b < kNumBuckets; ++b)
+            warp_append(q.bucket[b], &c->bucket[b], bucket == b, slot, q.capacity, &c->error);
+        warp_append(q.freeStack, &c->freeCount, miss, slot, q.capacity, &c->error);
+    }
+}
+
+__global__ void __launch_bounds__(kTraceBlock) k_trace_shadow(DevScene s, Queues q, PathSoA p) {
+    __shared__ uint2 sstack[kStackSmem * kTraceBlock];
+    Counters* c = q.ctr;
+    const uint32_t cur = c->cur;
+    const uint32_t n = min(c->shd[cur], q.capacity);
+    const uint32_t* in = q.shd[cur];
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        uint32_t i = base + threadIdx.x;
+        uint32_t slot = i < n ? in[i] : kInvalidSlot;
+        if (slot != kInvalidSlot && slot >= q.capacity) {
+            atomicOr(&c->error, kErrBadIndex);
+            slot = kInvalidSlot;
+        }
+        bool valid = slot != kInvalidSlot;
+        if (valid) {
+            float4 o = p.sh_o[slot], d = p.sh_d[slot];
+            Ray r{o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w};
+            float t;
+            uint32_t prim, mat;
+            // Shadow stage of __raygen__trace (trace.cu:27-51): add the NEE contribution if unoccluded.
+            if (!traverse<true>(s, r, t, prim, mat, sstack, &c->error)) {
+                float4 rd = p.rad[slot], cc = p.sh_c[slot];
+                p.rad[slot] = make_float4(rd.x + cc.x, rd.y + cc.y, rd.z + cc.z, rd.w);
+            }
+        }
+        warp_count64(&c->shdRays, valid);
+        warp_append(q.bucket[kBucketLambert], &c->bucket[kBucketLambert], valid, slot, q.capacity, &c->error);
+    }
+}
+
+void launch_trace_extension(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid,
+                            cudaStream_t st) {
+    k_trace_extension<<<grid, kTraceBlock, 0, st>>>(s, q, p, f);
+}
+void launch_trace_shadow(const DevScene& s, const Queues& q, const PathSoA& p, int grid, cudaStream_t st) {
+    k_trace_shadow<<<grid, kTraceBlock, 0, st>>>(s, q, p);
+}
+
+}  // namespace wrk

@@ -1,0 +1,428 @@
+// Drop-in C++ API (include/wr/*.h) on top of the C ABI (include/wrk.h).
+//
+// Mirrors libWR's public classes (trianglestrip/OfflineRenderer,
+// libWR/src/internal/{context,scene,renderer}.cpp): materials are appended with
+// libWR's defaults, meshes are accumulated as one flat triangle soup (indices
+// rebased, absent normals / uvs zero-padded), and finalize() hands everything to
+// libwrk, which builds the light CDF and the BVH on the GPU.  Failures of the C
+// ABI are rethrown as std::runtime_error, libWR's error convention
+// (libWR/src/internal/cuda_utils.h:13-39).
+#include <zlib.h>
+
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iterator>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/wr/wr.h"
+#include "../../include/wrk.h"
+
+namespace wr {
+namespace {
+
+void check(int rc, const char* what) {
+    if (rc != WRK_OK) throw std::runtime_error(std::string("wrk error in ") + what + ": " + wrk_last_error());
+}
+
+std::vector<uint8_t> read_file(const std::string& path) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) throw std::runtime_error("Failed to open: " + path);
+    return std::vector<uint8_t>(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+}
+
+uint32_t be32(const uint8_t* p) { return (uint32_t)p[0] << 24 | (uint32_t)p[1] << 16 | (uint32_t)p[2] << 8 | p[3]; }
+
+// PNG -> RGBA8: 8-bit grey / grey+alpha / RGB / RGBA / palette, non-interlaced.
+void decode_png(const std::vector<uint8_t>& d, std::vector<uint8_t>& rgba, uint32_t& w, uint32_t& h) {
+    static const uint8_t sig[8] = {0x89, 'P', 'N', 'G', 0x0d, 0x0a, 0x1a, 0x0a};
+    if (d.size() < 8 || std::memcmp(d.data(), sig, 8) != 0) throw std::runtime_error("not a PNG file");
+    size_t pos = 8;
+    uint8_t depth = 0, ctype = 0, interlace = 0;
+    std::vector<uint8_t> idat, plte, trns;
+    while (pos + 8 <= d.size()) {
+        uint32_t len = be32(&d[pos]);
+        std::string type(reinterpret_cast<const char*>(&d[pos + 4]), 4);
+        if (pos + 12 + (size_t)len > d.size()) throw std::runtime_error("truncated PNG");
+        const uint8_t* body = &d[pos + 8];
+        if (type == "IHDR") {
+            w = be32(body);
+            h = be32(body + 4);
+            depth = body[8];
+            ctype = body[9];
+            interlace = body[12];
+        } else if (type == "PLTE") {
+            plte.assign(body, body + len);
+        } else if (type == "tRNS") {
+            trns.assign(body, body + len);
+        } else if (type == "IDAT") {
+            idat.insert(idat.end(), body, body + len);
+        } else if (type == "IEND") {
+            break;
+        }
+        pos += 12 + len;
+    }
+    if (depth != 8 || interlace != 0) throw std::runtime_error("PNG: only 8-bit non-interlaced images are supported");
+    int ch = ctype == 0 ? 1 : ctype == 2 ? 3 : ctype == 3 ? 1 : ctype == 4 ? 2 : ctype == 6 ? 4 : 0;
+    if (!ch || w == 0 || h == 0) throw std::runtime_error("PNG: unsupported color type");
+    size_t stride = (size_t)w * ch;
+    std::vector<uint8_t> raw((stride + 1) * h);
+    uLongf rawLen = (uLongf)raw.size();
+    if (uncompress(raw.data(), &rawLen, idat.data(), (uLong)idat.size()) != Z_OK || rawLen != raw.size())
+        throw std::runtime_error("PNG: zlib stream error");
+    std::vector<uint8_t> img(stride * h), prev(stride, 0);
+    for (uint32_t y = 0; y < h; ++y) {
+        uint8_t f = raw[y * (stride + 1)];
+        const uint8_t* in = &raw[y * (stride + 1) + 1];
+        uint8_t* out = &img[y * stride];
+        for (size_t x = 0; x < stride; ++x) {
+            int a = x >= (size_t)ch ? out[x - ch] : 0, b = prev[x], c = x >= (size_t)ch ? prev[x - ch] : 0;
+            int v = in[x];
+            if (f == 1) v += a;
+            else if (f == 2) v += b;
+            else if (f == 3) v += (a + b) >> 1;
+            else if (f == 4) {
+                int p = a + b - c, pa = std::abs(p - a), pb = std::abs(p - b), pc = std::abs(p - c);
+                v += (pa <= pb && pa <= pc) ? a : (pb <= pc ? b : c);
+            }
+            out[x] = (uint8_t)v;
+        }
+        std::memcpy(prev.data(), out, stride);
+    }
+    rgba.resize((size_t)w * h * 4);
+    for (size_t i = 0; i < (size_t)w * h; ++i) {
+        uint8_t* o = &rgba[4 * i];
+        const uint8_t* s = &img[i * ch];
+        switch (ctype) {
+            case 0: o[0] = o[1] = o[2] = s[0]; o[3] = 255; break;
+            case 2: o[0] = s[0]; o[1] = s[1]; o[2] = s[2]; o[3] = 255; break;
+            case 3: {
+                size_t k = s[0];
+                if (3 * k + 2 >= plte.size()) throw std::runtime_error("PNG: palette index out of range");
+                o[0] = plte[3 * k]; o[1] = plte[3 * k + 1]; o[2] = plte[3 * k + 2];
+                o[3] = k < trns.size() ? trns[k] : 255;
+                break;
+            }
+            case 4: o[0] = o[1] = o[2] = s[0]; o[3] = s[1]; break;
+            default: o[0] = s[0]; o[1] = s[1]; o[2] = s[2]; o[3] = s[3]; break;
+        }
+    }
+}
+
+// Radiance .hdr (RGBE, flat or new-style run-length scanlines) -> RGBA float.
+void decode_hdr(const std::vector<uint8_t>& d, std::vector<float>& rgba, uint32_t& w, uint32_t& h) {
+    size_t pos = 0;
+    auto line = [&]() {
+        std::string s;
+        while (pos < d.size() && d[pos] != '\n') s += (char)d[pos++];
+        ++pos;
+        return s;
+    };
+    std::string l = line();
+    if (l.rfind("#?", 0) != 0) throw std::runtime_error("not a Radiance HDR file");
+    while (pos < d.size() && !(l = line()).empty()) {
+    }
+    l = line();
+    int H = 0, W = 0;
+    if (std::sscanf(l.c_str(), "-Y %d +X %d", &H, &W) != 2 || W <= 0 || H <= 0)
+        throw std::runtime_error("HDR: unsupported orientation");
+    w = (uint32_t)W;
+    h = (uint32_t)H;
+    std::vector<uint8_t> rgbe((size_t)W * H * 4);
+    for (int y = 0; y < H; ++y) {
+        uint8_t* row = &rgbe[(size_t)y * W * 4];
+        if (pos + 4 <= d.size() && d[pos] == 2 && d[pos + 1] == 2 && W >= 8 && W < 32768) {
+            pos += 4;
+            for (int c = 0; c < 4; ++c)
+                for (int x = 0; x < W;) {
+                    if (pos >= d.size()) throw std::runtime_error("HDR: truncated");
+                    int n = d[pos++];
+                    if (n > 128) {
+                        n -= 128;
+                        uint8_t v = d[pos++];
+                        for (int k = 0; k < n && x < W; ++k) row[4 * x++ + c] = v;
+                    } else {
+                        for (int k = 0; k < n && x < W; ++k) row[4 * x++ + c] = d[pos++];
+                    }
+                }
+        } else {
+            if (pos + (size_t)W * 4 > d.size()) throw std::runtime_error("HDR: truncated");
+            std::memcpy(row, &d[pos], (size_t)W * 4);
+            pos += (size_t)W * 4;
+        }
+    }
+    rgba.resize((size_t)W * H * 4);
+    for (size_t i = 0; i < (size_t)W * H; ++i) {
+        const uint8_t* e = &rgbe[4 * i];
+        float f = e[3] ? std::ldexp(1.0f, (int)e[3] - 136) : 0.0f;
+        rgba[4 * i] = e[0] * f;
+        rgba[4 * i + 1] = e[1] * f;
+        rgba[4 * i + 2] = e[2] * f;
+        rgba[4 * i + 3] = 1.0f;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+Context::Context(const ContextConfig& config) : m_device(config.deviceId) {
+    int n = 0;
+    check(wrk_device_count(&n), "Context");
+    if (n == 0) throw std::runtime_error("wrk: no CUDA device available");
+    if (m_device < 0 || m_device >= n) throw std::runtime_error("wrk: device id out of range");
+}
+Context::~Context() {}
+Scene* Context::createScene() { return new Scene(m_device); }
+Renderer* Context::createRenderer() { return new Renderer(RendererConfig{}, m_device); }
+int Context::getDeviceId() const { return m_device; }
+
+// ---------------------------------------------------------------------------
+struct SceneImpl {
+    int device = 0;
+    std::vector<float> vertices, normals, uvs;
+    std::vector<uint32_t> indices, triMat;
+    std::vector<wrk_material> materials;
+    std::vector<std::vector<uint8_t>> textures;
+    std::vector<uint32_t> texW, texH;
+    std::vector<float> envMap;
+    uint32_t envW = 0, envH = 0;
+    Vec3 env{0, 0, 0};
+    bool hasNormals = false, hasUVs = false, finalized = false;
+    wrk_scene* handle = nullptr;
+    wrk_scene_buffers bufs{};
+    ~SceneImpl() {
+        if (handle) wrk_scene_destroy(handle);
+    }
+    uint32_t add(const wrk_material& m) {
+        materials.push_back(m);
+        return (uint32_t)materials.size() - 1;
+    }
+};
+
+static wrk_material make_material(uint32_t type, const Vec3& albedo, const Vec3& emission, float ior, float rough,
+                                  float metal, uint32_t tex) {
+    wrk_material m{};
+    m.albedo[0] = albedo.x;
+    m.albedo[1] = albedo.y;
+    m.albedo[2] = albedo.z;
+    m.emission[0] = emission.x;
+    m.emission[1] = emission.y;
+    m.emission[2] = emission.z;
+    m.ior = ior;
+    m.type = type;
+    m.roughness = rough;
+    m.metallic = metal;
+    m.albedoTextureId = tex;
+    return m;
+}
+
+Scene::Scene() : m_impl(new SceneImpl()) {}
+Scene::Scene(int deviceId) : m_impl(new SceneImpl()) { m_impl->device = deviceId; }
+Scene::~Scene() { delete m_impl; }
+
+// Material defaults as libWR's Scene (scene.cpp:91-168).
+uint32_t Scene::addLambertianMaterial(const Vec3& albedo) { return addLambertianMaterial(albedo, 0); }
+uint32_t Scene::addLambertianMaterial(const Vec3& albedo, uint32_t tex) {
+    return m_impl->add(make_material(WRK_LAMBERTIAN, albedo, Vec3(0, 0, 0), 1.0f, 1.0f, 0.0f, tex));
+}
+uint32_t Scene::addEmissiveMaterial(const Vec3& emission) {
+    return m_impl->add(make_material(WRK_EMISSIVE, Vec3(0, 0, 0), emission, 1.0f, 0.0f, 0.0f, 0));
+}
+uint32_t Scene::addGlassMaterial(const Vec3& albedo, float ior) {
+    return m_impl->add(make_material(WRK_GLASS, albedo, Vec3(0, 0, 0), ior, 0.0f, 0.0f, 0));
+}
+uint32_t Scene::addGGXReflectionMaterial(const Vec3& albedo, float roughness, float metallic) {
+    return m_impl->add(make_material(WRK_GGX_REFLECTION, albedo, Vec3(0, 0, 0), 1.5f, roughness, metallic, 0));
+}
+uint32_t Scene::addGGXTransmissionMaterial(const Vec3& albedo, float roughness, float ior) {
+    return m_impl->add(make_material(WRK_GGX_TRANSMISSION, albedo, Vec3(0, 0, 0), ior, roughness, 0.0f, 0));
+}
+void Scene::setMaterialNormalMap(uint32_t materialId, uint32_t normalTextureId) {
+    if (materialId >= m_impl->materials.size()) throw std::runtime_error("Invalid material ID");
+    m_impl->materials[materialId].normalTextureId = normalTextureId;
+}
+
+void Scene::addTriangleMesh(std::span<const float> v, std::span<const uint32_t> i, uint32_t mat) {
+    addTriangleMesh(v, i, std::span<const float>(), std::span<const float>(), mat);
+}
+void Scene::addTriangleMesh(std::span<const float> v, std::span<const uint32_t> i, std::span<const float> uv,
+                            uint32_t mat) {
+    addTriangleMesh(v, i, std::span<const float>(), uv, mat);
+}
+// scene.cpp:190-244: indices rebased by the vertex offset, normals / uvs padded with
+// zeros for meshes that do not supply them, one material id per triangle.
+void Scene::addTriangleMesh(std::span<const float> v, std::span<const uint32_t> idx, std::span<const float> nrm,
+                            std::span<const float> uv, uint32_t mat) {
+    SceneImpl& s = *m_impl;
+    if (s.finalized) throw std::runtime_error("Scene already finalized");
+    uint32_t off = (uint32_t)(s.vertices.size() / 3);
+    size_t nv = v.size() / 3;
+    s.vertices.insert(s.vertices.end(), v.begin(), v.begin() + 3 * nv);
+    if (!nrm.empty() && nrm.size() >= nv * 3) {
+        s.hasNormals = true;
+        s.normals.insert(s.normals.end(), nrm.begin(), nrm.begin() + 3 * nv);
+    } else {
+        s.normals.insert(s.normals.end(), 3 * nv, 0.0f);
+    }
+    if (!uv.empty() && uv.size() >= nv * 2) {
+        s.hasUVs = true;
+        s.uvs.insert(s.uvs.end(), uv.begin(), uv.begin() + 2 * nv);
+    } else {
+        s.uvs.insert(s.uvs.end(), 2 * nv, 0.0f);
+    }
+    size_t nt = idx.size() / 3;
+    for (size_t k = 0; k < 3 * nt; ++k) s.indices.push_back(off + idx[k]);
+    s.triMat.insert(s.triMat.end(), nt, mat);
+}
+
+void Scene::setEnvironmentRadiance(const Vec3& r) { m_impl->env = r; }
+void Scene::setEnvironmentMap(const std::string& path) {
+    decode_hdr(read_file(path), m_impl->envMap, m_impl->envW, m_impl->envH);
+}
+
+uint32_t Scene::loadTexture(const std::string& path) {
+    std::vector<uint8_t> rgba;
+    uint32_t w = 0, h = 0;
+    try {
+        decode_png(read_file(path), rgba, w, h);
+    } catch (const std::exception& e) {
+        throw std::runtime_error("Failed to load texture: " + path + " (" + e.what() + ")");
+    }
+    return addTexture(rgba.data(), w, h);
+}
+uint32_t Scene::addTexture(const uint8_t* rgba, uint32_t w, uint32_t h) {
+    if (m_impl->finalized) throw std::runtime_error("Scene already finalized");
+    m_impl->textures.emplace_back(rgba, rgba + (size_t)w * h * 4);
+    m_impl->texW.push_back(w);
+    m_impl->texH.push_back(h);
+    return (uint32_t)m_impl->textures.size();
+}
+// scene.cpp:266-275: the texture keeps its id; a destroyed texture samples as white.
+void Scene::destroyTexture(uint32_t id) {
+    if (id == 0 || id > m_impl->textures.size()) return;
+    m_impl->textures[id - 1].clear();
+}
+uint32_t Texture2D::create(Scene* scene, const std::string& path) { return scene->loadTexture(path); }
+void Texture2D::destroy(Scene* scene, uint32_t id) { scene->destroyTexture(id); }
+
+void Scene::finalize(const SceneBuildConfig&) {
+    SceneImpl& s = *m_impl;
+    if (s.finalized) return;
+    if (s.vertices.empty() || s.indices.empty()) throw std::runtime_error("Scene has no geometry");
+    check(wrk_scene_create(s.device, &s.handle), "wrk_scene_create");
+    check(wrk_scene_set_geometry(s.handle, s.vertices.data(), (uint32_t)(s.vertices.size() / 3),
+                                 s.hasNormals ? s.normals.data() : nullptr, s.hasUVs ? s.uvs.data() : nullptr,
+                                 s.indices.data(), (uint32_t)s.triMat.size(), s.triMat.data()),
+          "wrk_scene_set_geometry");
+    check(wrk_scene_set_materials(s.handle, s.materials.data(), (uint32_t)s.materials.size()),
+          "wrk_scene_set_materials");
+    for (size_t i = 0; i < s.textures.size(); ++i) {
+        uint32_t id = 0;
+        // a destroyed texture keeps its slot as a 1x1 white texel
+        static const uint8_t white[4] = {255, 255, 255, 255};
+        bool gone = s.textures[i].empty();
+        check(wrk_scene_add_texture(s.handle, gone ? white : s.textures[i].data(), gone ? 1 : s.texW[i],
+                                    gone ? 1 : s.texH[i], &id),
+              "wrk_scene_add_texture");
+    }
+    float env[3] = {s.env.x, s.env.y, s.env.z};
+    check(wrk_scene_set_environment(s.handle, env), "wrk_scene_set_environment");
+    check(wrk_scene_finalize(s.handle), "wrk_scene_finalize");
+    check(wrk_scene_buffers_get(s.handle, &s.bufs), "wrk_scene_buffers_get");
+    s.finalized = true;
+}
+
+DevicePtr Scene::getVerticesBuffer() const { return m_impl->bufs.vertices; }
+DevicePtr Scene::getNormalsBuffer() const { return m_impl->bufs.normals; }
+DevicePtr Scene::getIndicesBuffer() const { return m_impl->bufs.indices; }
+DevicePtr Scene::getTriangleMaterialIdsBuffer() const { return m_impl->bufs.triMaterial; }
+DevicePtr Scene::getMaterialsBuffer() const { return m_impl->bufs.materials; }
+TraversableHandle Scene::getGASHandle() const { return m_impl->bufs.bvhNodes; }
+uint32_t Scene::getNumMaterials() const { return (uint32_t)m_impl->materials.size(); }
+Vec3 Scene::getEnvironmentRadiance() const { return m_impl->env; }
+uint64_t Scene::getEnvironmentMapTexture() const { return 0; }
+uint32_t Scene::getEnvironmentMapWidth() const { return m_impl->envW; }
+uint32_t Scene::getEnvironmentMapHeight() const { return m_impl->envH; }
+DevicePtr Scene::getEmissiveTrianglesBuffer() const { return m_impl->bufs.emissive; }
+DevicePtr Scene::getEmissiveTriangleCDFBuffer() const { return m_impl->bufs.cdf; }
+uint32_t Scene::getNumEmissiveTriangles() const { return m_impl->bufs.numEmissive; }
+DevicePtr Scene::getTexturesBuffer() const { return m_impl->bufs.texels; }
+uint32_t Scene::getNumTextures() const { return (uint32_t)m_impl->textures.size(); }
+DevicePtr Scene::getUVsBuffer() const { return m_impl->bufs.uvs; }
+wrk_scene* Scene::native() const { return m_impl->handle; }
+
+// ---------------------------------------------------------------------------
+struct RendererImpl {
+    int device = 0;
+    wrk_renderer* handle = nullptr;
+    RenderStats stats;
+    ~RendererImpl() {
+        if (handle) wrk_renderer_destroy(handle);
+    }
+};
+
+Renderer::Renderer(const RendererConfig& config) : Renderer(config, 0) {}
+Renderer::Renderer(const RendererConfig& config, int deviceId) : m_impl(new RendererImpl()), m_config(config) {
+    m_impl->device = deviceId;
+    try {
+        check(wrk_renderer_create(deviceId, 0, &m_impl->handle), "wrk_renderer_create");
+    } catch (...) {
+        delete m_impl;
+        throw;
+    }
+}
+Renderer::~Renderer() { delete m_impl; }
+const RenderStats& Renderer::lastStats() const { return m_impl->stats; }
+
+void Renderer::render(Scene* scene, const Camera& camera, Vec3* out, const RenderParams& p) {
+    if (!scene || !out) throw std::runtime_error("render: null scene or output buffer");
+    if (p.denoiser.enabled)
+        throw std::runtime_error("render: the denoise stage is not available in this build (render without it)");
+    scene->finalize();
+    wrk_camera c{};
+    c.position[0] = camera.position.x; c.position[1] = camera.position.y; c.position[2] = camera.position.z;
+    c.target[0] = camera.target.x; c.target[1] = camera.target.y; c.target[2] = camera.target.z;
+    c.up[0] = camera.up.x; c.up[1] = camera.up.y; c.up[2] = camera.up.z;
+    c.fovY = camera.fovY;
+    c.aspect = camera.aspect;
+    c.focalDistance = camera.focalDistance;
+    c.lensRadius = camera.lensRadius;
+    wrk_render_params rp{};
+    rp.width = p.width;
+    rp.height = p.height;
+    rp.spp = p.spp;
+    rp.useNEE = p.useNEE ? 1u : 0u;
+    rp.maxBounces = p.maxBounces;
+    rp.russianRouletteDepth = p.russianRouletteDepth;
+    rp.fireflyClamp = p.fireflyClamp;
+    rp.seed = p.seed;
+    rp.maxIterations = p.maxIterations;
+    rp.flags = p.rawGuides ? WRK_FLAG_RAW_GUIDES : 0u;
+    wrk_render_stats st{};
+    check(wrk_render(m_impl->handle, scene->native(), &c, &rp, reinterpret_cast<float*>(out),
+                     reinterpret_cast<float*>(p.albedoOut), reinterpret_cast<float*>(p.normalOut), &st),
+          "wrk_render");
+    m_impl->stats.paths = st.paths;
+    m_impl->stats.extensionRays = st.extensionRays;
+    m_impl->stats.shadowRays = st.shadowRays;
+    m_impl->stats.iterations = st.iterations;
+    m_impl->stats.gpuMs = st.gpuMs;
+    m_impl->stats.totalMs = st.totalMs;
+}
+
+// renderer.cpp:318-335
+void Renderer::render(Scene* scene, const Camera& camera, Vec3* out, uint32_t width, uint32_t height, uint32_t spp,
+                      bool denoiser) {
+    RenderParams p;
+    p.width = width;
+    p.height = height;
+    p.spp = spp;
+    p.denoiser.enabled = denoiser;
+    p.denoiser.useAlbedo = true;
+    p.denoiser.useNormal = true;
+    render(scene, camera, out, p);
+}
+
+}  // namespace wr

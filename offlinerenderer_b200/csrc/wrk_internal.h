@@ -1,0 +1,145 @@
+// Internal device-side layouts of libwrk (not part of the C ABI).
+//
+// HBM layout
+//   Scene (resident):  vertices / normals / uvs / indices / per-triangle material
+//                      (the flat soup libWR uploads, scene.cpp:360-390), 64 B materials,
+//                      RGBA8 texels, emissive list + power CDF, the 8-wide BVH
+//                      (80 B nodes = 5 x uint4) and leaf-ordered triangle records
+//                      (48 B = 3 x float4: v0|prim, e1|material, e2).
+//   Path slots (SoA, one float4 / uint4 per field, 16-byte aligned so every access
+//   is one 16-byte vector load or store):
+//      ray_o (origin, tmin)   ray_d (direction, tmax)   hit (t, prim, material, -)
+//      thr (throughput, prevPdf)   rad (radiance, pixel)   st (seed, rngDim, depth|iter<<16, flags|sample<<8)
+//      sh_o / sh_d (shadow ray)    sh_c (NEE contribution)
+//   Queues: u32 slot lists -- extension and shadow queues (double-buffered across
+//   iterations), four material buckets, and the free-slot stack.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/wrk.h"
+
+namespace wrk {
+
+enum : uint32_t { kLambert = 0, kEmissive = 1, kGlass = 2, kGGX = 3, kGGXT = 4 };
+// Material buckets the trace kernel sorts hits into.
+enum : uint32_t { kBucketLambert = 0, kBucketDielectric = 1, kBucketGGX = 2, kBucketOther = 3, kNumBuckets = 4 };
+// st.w flags
+enum : uint32_t { kFlagFirstHit = 1u, kFlagPrevDelta = 2u, kFlagNeeDone = 4u };
+
+constexpr uint32_t kInvalidSlot = 0xffffffffu;
+constexpr uint32_t kNoHit = 0xffffffffu;
+
+// Device error bits (Counters::error).
+enum : uint32_t { kErrStackOverflow = 1u, kErrBadIndex = 2u, kErrQueueOverflow = 4u };
+
+struct TexInfo {
+    uint64_t offset;  // byte offset into the texel pool
+    uint32_t w, h;
+};
+
+struct DevScene {
+    const float* vtx;
+    const float* nrm;  // null when no mesh supplied normals
+    const float* uv;   // null when no mesh supplied uvs
+    const uint32_t* idx;
+    const uint32_t* triMat;
+    const wrk_material* mats;
+    uint32_t numMats;
+    const uint8_t* texels;
+    const TexInfo* tex;
+    uint32_t numTex;
+    const uint32_t* emissive;
+    const float* cdf;
+    uint32_t numEmissive;
+    uint32_t numTris;
+    float env[3];
+    const uint4* nodes;
+    const float4* tris;
+    uint32_t numNodes;
+};
+
+struct PathSoA {
+    float4* ray_o;
+    float4* ray_d;
+    float4* hit;
+    float4* thr;
+    float4* rad;
+    uint4* st;
+    float4* sh_o;
+    float4* sh_d;
+    float4* sh_c;
+};
+
+// Queue counters and loop bookkeeping; lives in device memory, owned by the renderer.
+struct Counters {
+    uint32_t ext[2];
+    uint32_t shd[2];
+    uint32_t bucket[kNumBuckets];
+    uint32_t freeCount;
+    uint32_t cur;         // which ext/shd buffer the current iteration consumes
+    uint32_t genCount;    // paths generated this iteration
+    uint32_t genFreeBase; // free-stack index of the first slot popped this iteration
+    uint32_t genExtBase;  // extension-queue index where the generated paths go
+    uint32_t iteration;
+    unsigned long long nextWork;
+    unsigned long long totalWork;
+    unsigned long long genWorkBase;
+    unsigned long long extRays;
+    unsigned long long shdRays;
+    unsigned long long paths;
+    uint32_t error;
+    uint32_t pad;
+};
+
+struct Queues {
+    uint32_t* ext[2];
+    uint32_t* shd[2];
+    uint32_t* bucket[kNumBuckets];
+    uint32_t* freeStack;
+    Counters* ctr;
+    uint32_t capacity;
+};
+
+struct Frame {
+    float pos[3], fwd[3], right[3], up[3];
+    float tanHalf, aspect, focal, lens;
+    uint32_t width, height;
+    uint32_t tilesX, perSample;  // 8x4 pixel tiles; work items per sample (padded to whole tiles)
+    uint32_t spp, useNEE, maxBounces, seed, maxIter, sampleOffset;
+    float rrStart, fireflyClamp;
+    float4* accum;   // radiance sum per pixel
+    float4* albedo;  // first-hit albedo sum per pixel
+    float4* normal;  // first-hit normal sum per pixel
+    uint32_t* err;   // device error flags (Counters::error)
+};
+
+// ---- host-callable launchers (defined in the .cu files) ----
+void launch_control(const Queues& q, cudaStream_t st);
+void launch_generate(const Queues& q, const PathSoA& p, const Frame& f, int grid, cudaStream_t st);
+void launch_trace_extension(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid,
+                            cudaStream_t st);
+void launch_trace_shadow(const DevScene& s, const Queues& q, const PathSoA& p, int grid, cudaStream_t st);
+void launch_shade(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid, cudaStream_t st);
+void launch_shade_bucket(uint32_t bucket, const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f,
+                         int grid, cudaStream_t st);
+void launch_resolve(const Frame& f, uint32_t rawGuides, float* rgb, float* albedo, float* normal, cudaStream_t st);
+
+// BVH build (bvh_build.cu)
+struct BvhBuildResult {
+    uint4* nodes;
+    float4* tris;
+    uint32_t numNodes, numBinary, depth;
+    float ms;
+    float sah;
+};
+int build_bvh8(const float* d_vtx, const uint32_t* d_idx, const uint32_t* d_triMat, uint32_t numTris,
+               cudaStream_t st, BvhBuildResult* out, char* err, size_t errlen);
+
+// standalone ray queries (trace.cu)
+void launch_closest_query(const DevScene& s, const float* rays, uint32_t n, float* t, uint32_t* prim,
+                          uint32_t* err, cudaStream_t st);
+void launch_occluded_query(const DevScene& s, const float* rays, uint32_t n, uint32_t* occ, uint32_t* err,
+                           cudaStream_t st);
+
+}  // namespace wrk

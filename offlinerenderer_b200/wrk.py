@@ -1,0 +1,431 @@
+"""Python binding of libwrk.so (the C ABI in include/wrk.h), via ctypes.
+
+Mirrors libWR's public API (trianglestrip/OfflineRenderer, libWR/include/wr/*.h):
+``Scene`` with addLambertianMaterial / addEmissiveMaterial / addGlassMaterial /
+addGGXReflectionMaterial / addGGXTransmissionMaterial / setMaterialNormalMap /
+addTriangleMesh / setEnvironmentRadiance / finalize, and ``Renderer.render``.
+Errors raise ``WrkError`` (a RuntimeError, libWR's convention).  There is no CPU
+path: if libwrk.so is missing or no GPU is present, calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import os
+
+import numpy as np
+
+from . import scenes as _scenes
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwrk.so")
+
+WRK_FLAG_RAW_GUIDES = 1
+WRK_FLAG_STAGE_TIMING = 2
+STAGES = ["control", "generate", "trace_extension", "trace_shadow", "shade_lambert", "shade_dielectric", "shade_ggx",
+          "shade_emissive"]
+
+
+class WrkError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"wrk error {code}: {msg}")
+        self.code = code
+
+
+class Material(C.Structure):
+    _fields_ = [("albedo", C.c_float * 4), ("emission", C.c_float * 4), ("ior", C.c_float), ("type", C.c_uint32),
+                ("roughness", C.c_float), ("metallic", C.c_float), ("albedoTextureId", C.c_uint32),
+                ("normalTextureId", C.c_uint32), ("pad", C.c_uint32 * 2)]
+
+
+class CameraC(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("target", C.c_float * 3), ("up", C.c_float * 3), ("fovY", C.c_float),
+                ("aspect", C.c_float), ("focalDistance", C.c_float), ("lensRadius", C.c_float)]
+
+
+class RenderParamsC(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("useNEE", C.c_uint32),
+                ("maxBounces", C.c_uint32), ("russianRouletteDepth", C.c_float), ("fireflyClamp", C.c_float),
+                ("seed", C.c_uint32), ("maxIterations", C.c_uint32), ("flags", C.c_uint32),
+                ("sampleOffset", C.c_uint32)]
+
+
+class RenderStatsC(C.Structure):
+    _fields_ = [("paths", C.c_uint64), ("extensionRays", C.c_uint64), ("shadowRays", C.c_uint64),
+                ("iterations", C.c_uint32), ("deviceErrors", C.c_uint32), ("gpuMs", C.c_float),
+                ("totalMs", C.c_float), ("stageMs", C.c_float * 8), ("stageLaunches", C.c_uint32 * 8)]
+
+
+class BvhInfoC(C.Structure):
+    _fields_ = [("numTriangles", C.c_uint32), ("numNodes", C.c_uint32), ("numBinaryNodes", C.c_uint32),
+                ("depth", C.c_uint32), ("numEmissive", C.c_uint32), ("buildMs", C.c_float), ("sahCost", C.c_float)]
+
+
+# Every entry point include/wrk.h declares, with its ctypes signature.
+_VP, _U32, _U64, _I, _F = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_float
+SIGNATURES = {
+    "wrk_last_error": ([], C.c_char_p),
+    "wrk_version": ([], _I),
+    "wrk_device_count": ([C.POINTER(C.c_int)], _I),
+    "wrk_malloc": ([_I, _U64, C.POINTER(_VP)], _I),
+    "wrk_free": ([_VP], _I),
+    "wrk_memcpy_htod": ([_VP, _VP, _U64], _I),
+    "wrk_memcpy_dtoh": ([_VP, _VP, _U64], _I),
+    "wrk_synchronize": ([_I], _I),
+    "wrk_scene_create": ([_I, C.POINTER(_VP)], _I),
+    "wrk_scene_destroy": ([_VP], _I),
+    "wrk_scene_set_geometry": ([_VP, _VP, _U32, _VP, _VP, _VP, _U32, _VP], _I),
+    "wrk_scene_set_materials": ([_VP, _VP, _U32], _I),
+    "wrk_scene_add_texture": ([_VP, _VP, _U32, _U32, C.POINTER(_U32)], _I),
+    "wrk_scene_set_environment": ([_VP, _VP], _I),
+    "wrk_scene_finalize": ([_VP], _I),
+    "wrk_scene_bvh_info": ([_VP, C.POINTER(BvhInfoC)], _I),
+    "wrk_scene_light_cdf": ([_VP, _VP, _VP, _U32, C.POINTER(_U32)], _I),
+    "wrk_scene_buffers_get": ([_VP, _VP], _I),
+    "wrk_renderer_create": ([_I, _U32, C.POINTER(_VP)], _I),
+    "wrk_renderer_destroy": ([_VP], _I),
+    "wrk_render": ([_VP, _VP, C.POINTER(CameraC), C.POINTER(RenderParamsC), _VP, _VP, _VP,
+                    C.POINTER(RenderStatsC)], _I),
+    "wrk_render_device": ([_VP, _VP, C.POINTER(CameraC), C.POINTER(RenderParamsC), _VP, _VP, _VP,
+                           C.POINTER(RenderStatsC)], _I),
+    "wrk_trace_closest": ([_VP, _VP, _U32, _VP, _VP], _I),
+    "wrk_trace_occluded": ([_VP, _VP, _U32, _VP], _I),
+    "wrk_compact": ([_VP, _VP, _U32, _VP, _VP], _I),
+    "wrk_cdf_sample": ([_VP, _U32, _VP, _U32, _VP], _I),
+    "wrk_rng_batch": ([_VP, _VP, _U32, _VP, _VP], _I),
+    "wrk_bsdf_batch": ([_VP, _U32, _VP], _I),
+    "wrk_texture_batch": ([_VP, _U32, _VP, _U32, _VP], _I),
+    "wrk_camera_rays": ([C.POINTER(CameraC), _U32, _U32, _VP, _VP, _U32, _U32, _VP], _I),
+    "wrk_tonemap_aces": ([_VP, _U32, _VP], _I),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libwrk.so (built in-tree by offlinerenderer_b200.build); raises if absent."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m offlinerenderer_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise WrkError(rc, lib().wrk_last_error().decode())
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    _check(lib().wrk_device_count(C.byref(n)))
+    return n.value
+
+
+class DeviceArray:
+    """Device memory from wrk_malloc holding one numpy-typed array."""
+
+    def __init__(self, shape, dtype, device: int = 0):
+        self.shape = tuple(np.atleast_1d(shape)) if not isinstance(shape, tuple) else shape
+        self.dtype = np.dtype(dtype)
+        self.nbytes = int(np.prod(self.shape)) * self.dtype.itemsize
+        p = C.c_void_p()
+        _check(lib().wrk_malloc(device, max(1, self.nbytes), C.byref(p)))
+        self.ptr = p.value
+
+    @classmethod
+    def from_numpy(cls, a: np.ndarray, device: int = 0) -> "DeviceArray":
+        a = np.ascontiguousarray(a)
+        d = cls(a.shape, a.dtype, device)
+        if d.nbytes:
+            _check(lib().wrk_memcpy_htod(d.ptr, a.ctypes.data, d.nbytes))
+        return d
+
+    def numpy(self) -> np.ndarray:
+        out = np.empty(self.shape, self.dtype)
+        if self.nbytes:
+            _check(lib().wrk_memcpy_dtoh(out.ctypes.data, self.ptr, self.nbytes))
+        return out
+
+    def __del__(self):
+        p = getattr(self, "ptr", None)
+        if p and _lib is not None:
+            _lib.wrk_free(p)
+            self.ptr = None
+
+
+def camera_struct(cam) -> CameraC:
+    c = CameraC()
+    c.position[:] = tuple(cam.position)
+    c.target[:] = tuple(cam.target)
+    c.up[:] = tuple(cam.up)
+    c.fovY, c.aspect = cam.fovY, cam.aspect
+    c.focalDistance, c.lensRadius = cam.focalDistance, cam.lensRadius
+    return c
+
+
+def params_struct(st, spp=None, max_iterations=8, raw_guides=False, seed=None, sample_offset=0,
+                  stage_timing=False) -> RenderParamsC:
+    p = RenderParamsC()
+    p.width, p.height = st.width, st.height
+    p.spp = st.spp if spp is None else spp
+    p.useNEE = 1 if st.useNEE else 0
+    p.maxBounces = st.maxBounces
+    p.russianRouletteDepth = st.russianRouletteDepth
+    p.fireflyClamp = st.fireflyClamp
+    p.seed = st.seed if seed is None else seed
+    p.maxIterations = max_iterations
+    p.flags = (WRK_FLAG_RAW_GUIDES if raw_guides else 0) | (WRK_FLAG_STAGE_TIMING if stage_timing else 0)
+    p.sampleOffset = sample_offset
+    return p
+
+
+def _stats_dict(stats: "RenderStatsC") -> dict:
+    d = {k: getattr(stats, k) for k, _ in RenderStatsC._fields_ if k not in ("stageMs", "stageLaunches")}
+    d["stageMs"] = {n: stats.stageMs[i] for i, n in enumerate(STAGES)}
+    d["stageLaunches"] = {n: stats.stageLaunches[i] for i, n in enumerate(STAGES)}
+    return d
+
+
+class Scene:
+    """wr::Scene: materials and meshes are accumulated on the host; finalize()
+    uploads them, builds the light CDF and the GPU BVH."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        self._b = _scenes._Builder()
+        self._env = (0.0, 0.0, 0.0)
+        self.handle = None
+
+    # material creation with libWR's defaults (scene.cpp:91-168)
+    def addLambertianMaterial(self, albedo, albedoTextureId: int = 0) -> int:
+        return self._b.lambertian(tuple(albedo), albedoTextureId)
+
+    def addEmissiveMaterial(self, emission) -> int:
+        return self._b.emissive(tuple(emission))
+
+    def addGlassMaterial(self, albedo, ior: float) -> int:
+        return self._b.glass(tuple(albedo), ior)
+
+    def addGGXReflectionMaterial(self, albedo, roughness: float, metallic: float = 0.0) -> int:
+        return self._b.ggx(tuple(albedo), roughness, metallic)
+
+    def addGGXTransmissionMaterial(self, albedo, roughness: float, ior: float) -> int:
+        return self._b.ggx_transmission(tuple(albedo), roughness, ior)
+
+    def setMaterialNormalMap(self, materialId: int, normalTextureId: int) -> None:
+        if materialId >= len(self._b.mats):
+            raise WrkError(1, "Invalid material ID")
+        self._b.mats[materialId]["normalTextureId"] = normalTextureId
+
+    def addTexture(self, rgba: np.ndarray) -> int:
+        """RGBA8 (H, W, 4) texture; returns the 1-based id (Texture2D::create)."""
+        return self._b.texture(rgba)
+
+    def addTriangleMesh(self, vertices, indices, materialId: int, normals=None, uvs=None) -> None:
+        self._b.mesh(vertices, indices, materialId, normals=normals, uvs=uvs)
+
+    def setEnvironmentRadiance(self, rgb) -> None:
+        self._env = tuple(float(x) for x in rgb)
+
+    @classmethod
+    def from_data(cls, sd: "_scenes.SceneData", device: int = 0) -> "Scene":
+        s = cls(device)
+        s._data = sd
+        s._finalize_data(sd)
+        return s
+
+    def finalize(self) -> None:
+        if self.handle is not None:
+            return
+        if not self._b.v:
+            raise WrkError(1, "Scene has no geometry")
+        sd = self._b.build(env=self._env)
+        self._data = sd
+        self._finalize_data(sd)
+
+    def _finalize_data(self, sd) -> None:
+        L = lib()
+        h = C.c_void_p()
+        _check(L.wrk_scene_create(self.device, C.byref(h)))
+        self.handle = h.value
+        v = np.ascontiguousarray(sd.vertices, np.float32)
+        idx = np.ascontiguousarray(sd.indices, np.uint32)
+        tm = np.ascontiguousarray(sd.tri_material, np.uint32)
+        nrm = None if sd.normals is None else np.ascontiguousarray(sd.normals, np.float32)
+        uv = None if sd.uvs is None else np.ascontiguousarray(sd.uvs, np.float32)
+        _check(L.wrk_scene_set_geometry(self.handle, v.ctypes.data, v.shape[0], None if nrm is None else nrm.ctypes.data,
+                                        None if uv is None else uv.ctypes.data, idx.ctypes.data, idx.shape[0],
+                                        tm.ctypes.data))
+        mats = np.ascontiguousarray(sd.materials)
+        _check(L.wrk_scene_set_materials(self.handle, mats.ctypes.data, mats.shape[0]))
+        for t in sd.textures:
+            t = np.ascontiguousarray(t, np.uint8)
+            tid = C.c_uint32()
+            _check(L.wrk_scene_add_texture(self.handle, t.ctypes.data, t.shape[1], t.shape[0], C.byref(tid)))
+        env = np.asarray(sd.env, np.float32)
+        _check(L.wrk_scene_set_environment(self.handle, env.ctypes.data))
+        _check(L.wrk_scene_finalize(self.handle))
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and _lib is not None:
+            _lib.wrk_scene_destroy(h)
+            self.handle = None
+
+    def bvh_info(self) -> dict:
+        info = BvhInfoC()
+        _check(lib().wrk_scene_bvh_info(self.handle, C.byref(info)))
+        return {k: getattr(info, k) for k, _ in BvhInfoC._fields_}
+
+    def light_cdf(self):
+        n = C.c_uint32()
+        _check(lib().wrk_scene_light_cdf(self.handle, None, None, 0, C.byref(n)))
+        tris = np.zeros(n.value, np.uint32)
+        cdf = np.zeros(n.value, np.float32)
+        _check(lib().wrk_scene_light_cdf(self.handle, tris.ctypes.data, cdf.ctypes.data, n.value, C.byref(n)))
+        return tris, cdf
+
+    def trace_closest(self, rays: np.ndarray):
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        dr = DeviceArray.from_numpy(rays, self.device)
+        dt = DeviceArray((n,), np.float32, self.device)
+        dp = DeviceArray((n,), np.uint32, self.device)
+        _check(lib().wrk_trace_closest(self.handle, dr.ptr, n, dt.ptr, dp.ptr))
+        return dt.numpy(), dp.numpy()
+
+    def trace_occluded(self, rays: np.ndarray):
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        dr = DeviceArray.from_numpy(rays, self.device)
+        do = DeviceArray((n,), np.uint32, self.device)
+        _check(lib().wrk_trace_occluded(self.handle, dr.ptr, n, do.ptr))
+        return do.numpy()
+
+    def texture_batch(self, texture_id: int, uv: np.ndarray) -> np.ndarray:
+        uv = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+        n = uv.shape[0]
+        du = DeviceArray.from_numpy(uv, self.device)
+        do = DeviceArray((n, 4), np.float32, self.device)
+        _check(lib().wrk_texture_batch(self.handle, texture_id, du.ptr, n, do.ptr))
+        return do.numpy()
+
+
+@dataclasses.dataclass
+class RenderResult:
+    rgb: np.ndarray
+    albedo: np.ndarray | None
+    normal: np.ndarray | None
+    stats: dict
+
+
+class Renderer:
+    """wr::Renderer: one CUDA stream and a pool of ``capacity`` path slots."""
+
+    def __init__(self, device: int = 0, capacity: int = 0):
+        self.device = device
+        h = C.c_void_p()
+        _check(lib().wrk_renderer_create(device, capacity, C.byref(h)))
+        self.handle = h.value
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and _lib is not None:
+            _lib.wrk_renderer_destroy(h)
+            self.handle = None
+
+    def render(self, scene: Scene, camera=None, settings=None, spp=None, guides=True, raw_guides=False,
+               max_iterations=8, seed=None, sample_offset=0, stage_timing=False) -> RenderResult:
+        """Synchronous render into host buffers (rgb = sum/spp, as libWR returns it)."""
+        cam = camera_struct(camera or scene._data.camera)
+        st = settings or scene._data.settings
+        p = params_struct(st, spp=spp, max_iterations=max_iterations, raw_guides=raw_guides, seed=seed,
+                          sample_offset=sample_offset, stage_timing=stage_timing)
+        shape = (st.height, st.width, 3)
+        rgb = np.zeros(shape, np.float32)
+        alb = np.zeros(shape, np.float32) if guides else None
+        nrm = np.zeros(shape, np.float32) if guides else None
+        stats = RenderStatsC()
+        _check(lib().wrk_render(self.handle, scene.handle, C.byref(cam), C.byref(p), rgb.ctypes.data,
+                                None if alb is None else alb.ctypes.data, None if nrm is None else nrm.ctypes.data,
+                                C.byref(stats)))
+        return RenderResult(rgb, alb, nrm, _stats_dict(stats))
+
+    def render_device(self, scene: Scene, d_rgb: DeviceArray, camera=None, settings=None, spp=None,
+                      d_albedo: DeviceArray | None = None, d_normal: DeviceArray | None = None,
+                      max_iterations=8, seed=None, sample_offset=0, stage_timing=False, d_rgb_ptr=None) -> dict:
+        """Render into device buffers (inputs and outputs stay in HBM)."""
+        cam = camera_struct(camera or scene._data.camera)
+        st = settings or scene._data.settings
+        p = params_struct(st, spp=spp, max_iterations=max_iterations, seed=seed, sample_offset=sample_offset,
+                          stage_timing=stage_timing)
+        stats = RenderStatsC()
+        out_ptr = d_rgb_ptr if d_rgb_ptr is not None else d_rgb.ptr
+        _check(lib().wrk_render_device(self.handle, scene.handle, C.byref(cam), C.byref(p), out_ptr,
+                                       None if d_albedo is None else d_albedo.ptr,
+                                       None if d_normal is None else d_normal.ptr, C.byref(stats)))
+        return _stats_dict(stats)
+
+
+# ---- kernel-level entry points (numpy in / numpy out) ----
+def compact(stage: np.ndarray, idx: np.ndarray, device: int = 0) -> np.ndarray:
+    ds = DeviceArray.from_numpy(np.asarray(stage, np.uint32), device)
+    di = DeviceArray.from_numpy(np.asarray(idx, np.uint32), device)
+    do = DeviceArray((max(1, len(idx)),), np.uint32, device)
+    dc = DeviceArray((1,), np.uint32, device)
+    _check(lib().wrk_compact(ds.ptr, di.ptr, len(idx), do.ptr, dc.ptr))
+    return do.numpy()[: int(dc.numpy()[0])]
+
+
+def cdf_sample(cdf: np.ndarray, u: np.ndarray, device: int = 0) -> np.ndarray:
+    dc = DeviceArray.from_numpy(np.asarray(cdf, np.float32), device)
+    du = DeviceArray.from_numpy(np.asarray(u, np.float32), device)
+    do = DeviceArray((len(u),), np.uint32, device)
+    _check(lib().wrk_cdf_sample(dc.ptr, len(cdf), du.ptr, len(u), do.ptr))
+    return do.numpy()
+
+
+def rng_batch(seeds: np.ndarray, dims: np.ndarray, device: int = 0):
+    n = len(seeds)
+    ds = DeviceArray.from_numpy(np.asarray(seeds, np.uint32), device)
+    dd = DeviceArray.from_numpy(np.asarray(dims, np.uint32), device)
+    dh = DeviceArray((n,), np.uint32, device)
+    du = DeviceArray((n,), np.float32, device)
+    _check(lib().wrk_rng_batch(ds.ptr, dd.ptr, n, dh.ptr, du.ptr))
+    return dh.numpy(), du.numpy()
+
+
+def bsdf_batch(records: np.ndarray, device: int = 0) -> np.ndarray:
+    records = np.ascontiguousarray(records, np.float32).reshape(-1, 20)
+    n = records.shape[0]
+    di = DeviceArray.from_numpy(records, device)
+    do = DeviceArray((n, 34), np.float32, device)
+    _check(lib().wrk_bsdf_batch(di.ptr, n, do.ptr))
+    return do.numpy()
+
+
+def camera_rays(camera, width: int, height: int, pixels, samples, seed: int = 0, device: int = 0) -> np.ndarray:
+    pixels = np.asarray(pixels, np.uint32)
+    n = len(pixels)
+    dp = DeviceArray.from_numpy(pixels, device)
+    ds = DeviceArray.from_numpy(np.asarray(samples, np.uint32), device)
+    do = DeviceArray((n, 8), np.float32, device)
+    cam = camera_struct(camera)
+    _check(lib().wrk_camera_rays(C.byref(cam), width, height, dp.ptr, ds.ptr, n, seed, do.ptr))
+    return do.numpy()
+
+
+def tonemap_aces(rgb: np.ndarray, device: int = 0) -> np.ndarray:
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    npx = rgb.size // 3
+    di = DeviceArray.from_numpy(rgb, device)
+    do = DeviceArray(rgb.shape, np.uint8, device)
+    _check(lib().wrk_tonemap_aces(di.ptr, npx, do.ptr))
+    return do.numpy()

@@ -1,0 +1,60 @@
+"""The C ABI boundary without a GPU: libwrk.so loads, exports every entry point
+include/wrk.h declares (and the drop-in C++ API), and fails loudly -- with an
+error code and message, never a CPU fallback -- when no device is present."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+
+def declared_entry_points():
+    text = open(os.path.join(ROOT, "include", "wrk.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(wrk_\w+)\s*\(", text, re.M)))
+
+
+def test_header_declares_entry_points():
+    names = declared_entry_points()
+    assert "wrk_render" in names and "wrk_trace_closest" in names and len(names) >= 30
+
+
+def test_library_exports_every_declared_symbol(wrk_lib):
+    L = C.CDLL(wrk_lib.LIB_PATH)
+    missing = [n for n in declared_entry_points() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_every_declared_symbol(wrk_lib):
+    assert set(declared_entry_points()) == set(wrk_lib.SIGNATURES)
+
+
+def test_cpp_api_symbols_exported(wrk_lib):
+    out = subprocess.run(["nm", "-DC", "--defined-only", wrk_lib.LIB_PATH], capture_output=True, text=True).stdout
+    for sym in ["wr::Scene::addTriangleMesh(std::span<float const", "wr::Scene::finalize(wr::SceneBuildConfig const&)",
+                "wr::Renderer::render(wr::Scene*, wr::Camera const&, wr::Vec3*, wr::RenderParams const&)",
+                "wr::Context::createScene()", "wr::Texture2D::create(wr::Scene*",
+                "wr::Scene::addGGXTransmissionMaterial(wr::Vec3 const&, float, float)"]:
+        assert sym in out, sym
+
+
+def test_no_device_fails_loudly(wrk_lib):
+    import ctypes
+
+    if wrk_lib.device_count() > 0:
+        pytest.skip("a GPU is visible; this checks the no-GPU error path")
+    L = wrk_lib.lib()
+    h = ctypes.c_void_p()
+    rc = L.wrk_scene_create(0, ctypes.byref(h))
+    assert rc == 4  # WRK_ERR_NO_DEVICE
+    assert b"no CUDA device" in L.wrk_last_error()
+    with pytest.raises(wrk_lib.WrkError):
+        wrk_lib.Renderer()
+
+
+def test_invalid_arguments_rejected_without_device(wrk_lib):
+    L = wrk_lib.lib()
+    assert L.wrk_device_count(None) == 1  # WRK_ERR_INVALID
+    assert L.wrk_cdf_sample(None, 0, None, 0, None) == 1
