@@ -49,9 +49,15 @@ CONFIGS = {
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
-# Algorithmic bytes per extension ray for the trace kernel: read the ray
-# (origin|tmin, direction|tmax = 32 B) + write the hit record (t, prim, material = 16 B).
-TRACE_BYTES_PER_RAY = 48
+# Algorithmic HBM bytes per unit of work of each loop stage (per path, per ray):
+#   trace_extension: read the ray (origin|tmin, direction|tmax = 32 B) + write the
+#                    hit record (t, prim, material = 16 B)                      = 48 B / ray
+#   trace_shadow:    shadow ray 32 B + contribution 16 B read, radiance 16 B read
+#                    and written, 4 B queue entry (rounded as 100 B / shadow ray)
+#   shade_*:         read direction 16 + hit 16 + path state 48, write state 48 +
+#                    next ray 32                                                = 160 B / path
+STAGE_BYTES = {"trace_extension": 48, "trace_shadow": 100, "shade_lambert": 160, "shade_dielectric": 160,
+               "shade_ggx": 160, "shade_emissive": 160, "shade_lambert_resume": 160}
 
 
 class ClockSampler:
@@ -189,6 +195,7 @@ def main():
     ap.add_argument("--impl", default="wrk", choices=["wrk", "reference"])
     ap.add_argument("--config", default="showcase", choices=list(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--spp", type=int, default=0, help="override the config's spp (smaller profiling cases)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
@@ -214,6 +221,8 @@ def main():
 
     _b.build()
     sd = cfg["make"]()
+    if args.spp:
+        sd.settings.spp = args.spp
     st = sd.settings
     scene = wrk.Scene.from_data(sd, device=local)
     rend = wrk.Renderer(device=local)
@@ -260,12 +269,17 @@ def main():
     # per-stage device times (events on the renderer's stream), one extra render
     tst = rend.render_device(scene, None, d_rgb_ptr=frame.data_ptr(), stage_timing=True)
     stage_ms = tst["stageMs"]
-    dominant = max(stage_ms, key=lambda k: stage_ms[k])
-    tr_ms = stage_ms["trace_extension"]
-    tr_launches = max(1, tst["stageLaunches"]["trace_extension"])
-    tr_bytes = TRACE_BYTES_PER_RAY * tst["extensionRays"]
+    units = {"trace_extension": tst["extensionRays"], "trace_shadow": tst["shadowRays"],
+             "shade_lambert": tst["bucketPaths"]["lambert"], "shade_dielectric": tst["bucketPaths"]["dielectric"],
+             "shade_ggx": tst["bucketPaths"]["ggx"], "shade_emissive": tst["bucketPaths"]["other"],
+             "shade_lambert_resume": tst["bucketPaths"]["lambert_resume"]}
+    dominant = max(STAGE_BYTES, key=lambda k: stage_ms[k])
     peak, peak_kind = hbm_peak()
-    achieved = tr_bytes / (tr_ms / 1e3) / 1e9 if tr_ms > 0 else None
+    launches = max(1, tst["stageLaunches"][dominant])
+    dom_bytes = STAGE_BYTES[dominant] * units[dominant]
+    achieved = dom_bytes / (stage_ms[dominant] / 1e3) / 1e9 if stage_ms[dominant] > 0 else None
+    stage_gbs = {k: (STAGE_BYTES[k] * units[k] / (stage_ms[k] / 1e3) / 1e9 if stage_ms[k] > 0 else None)
+                 for k in STAGE_BYTES}
 
     # end to end through the public C ABI with host buffers
     e2e_steps = max(1, min(args.steps, 3))
@@ -308,14 +322,17 @@ def main():
                        "l2": "per-step working set (path slots 4M x 144 B = 604 MB) exceeds the 126 MB L2"},
             "mrays_per_s": mrays,
             "iterations_per_step": iters / args.steps,
-            "gpu_launches": iters * 8 + args.steps * 2,
+            "gpu_launches": iters * 9 + args.steps * 2,
             "e2e": {"value": e2e_val, "unit": "Msamples/s", "h2d_bytes_per_step": 76 + 44,
                     "d2h_bytes_per_step": npx * 3 * 4 * 3},
-            "roofline": {"bound": "hbm", "kernel": "k_trace_extension", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
-                         "peak_source": peak_kind, "avg_launch_ms": tr_ms / tr_launches,
-                         "algorithmic_bytes_per_launch": tr_bytes / tr_launches, "dominant_stage": dominant},
+                         "peak_source": peak_kind, "avg_launch_ms": stage_ms[dominant] / launches,
+                         "algorithmic_bytes_per_launch": dom_bytes / launches,
+                         "units_per_launch": units[dominant] / launches},
             "stage_ms": stage_ms,
+            "stage_algorithmic_gbs": stage_gbs,
+            "stage_units": units,
             "clocks": clk,
             "cpu_baseline": cpu,
         }

@@ -79,7 +79,8 @@ enum {
     WRK_STAGE_SHADE_DIELECTRIC = 5,
     WRK_STAGE_SHADE_GGX = 6,
     WRK_STAGE_SHADE_EMISSIVE = 7,
-    WRK_NUM_STAGES = 8
+    WRK_STAGE_SHADE_LAMBERT_RESUME = 8,
+    WRK_NUM_STAGES = 9
 };
 
 typedef struct {
@@ -90,8 +91,9 @@ typedef struct {
     uint32_t deviceErrors;   /* internal device error flags raised (0 = none) */
     float gpuMs;             /* device time of the render loop (CUDA events) */
     float totalMs;           /* device time including uploads / readback */
-    float stageMs[8];        /* per-stage device time (WRK_FLAG_STAGE_TIMING), indexed by WRK_STAGE_* */
-    uint32_t stageLaunches[8];
+    float stageMs[9];        /* per-stage device time (WRK_FLAG_STAGE_TIMING), indexed by WRK_STAGE_* */
+    uint32_t stageLaunches[9];
+    uint64_t bucketPaths[5]; /* paths shaded per bucket: Lambert, dielectric, GGX, emissive/other, Lambert resume */
 } wrk_render_stats;
 
 typedef struct {

@@ -489,21 +489,21 @@ static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, con
     CK(cudaMemsetAsync(f.accum, 0, np * 3 * sizeof(float4), st));
     Counters c0{};
     c0.cur = 1;
-    c0.freeCount = r->capacity;
+    c0.freeCount.v = r->capacity;
     c0.totalWork = (unsigned long long)np * p->spp;
     CK(cudaMemcpyAsync(r->q.ctr, &c0, sizeof(Counters), cudaMemcpyHostToDevice, st));
     k_iota<<<(r->capacity + 255) / 256, 256, 0, st>>>(r->q.freeStack, r->capacity);
     CK(cudaGetLastError());
-    const int traceGrid = r->numSMs * 6, shadeGrid = r->numSMs * 4;
+    const int traceGrid = r->numSMs * 8, shadeGrid = r->numSMs * 4;
     // bound on iterations: every path needs <= maxIter; waves of `capacity` paths
     unsigned long long waves = c0.totalWork / r->capacity + 2;
     unsigned long long maxIters = waves * (unsigned long long)(f.maxIter + 2) * 4ull + 64ull;
     uint32_t iters = 0;
     const uint32_t kChunk = 8;
     const bool timing = (p->flags & WRK_FLAG_STAGE_TIMING) != 0;
-    // one event before and after each of the 8 launches of an iteration
-    if (timing && r->stageEv.size() < kChunk * 9) {
-        while (r->stageEv.size() < kChunk * 9) {
+    // one event before and after each of the 9 launches of an iteration
+    if (timing && r->stageEv.size() < kChunk * 10) {
+        while (r->stageEv.size() < kChunk * 10) {
             cudaEvent_t e;
             CK(cudaEventCreate(&e));
             r->stageEv.push_back(e);
@@ -514,7 +514,7 @@ static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, con
     CK(cudaEventRecord(r->evLoop0, st));
     while (true) {
         for (uint32_t k = 0; k < kChunk; ++k) {
-            cudaEvent_t* ev = timing ? &r->stageEv[k * 9] : nullptr;
+            cudaEvent_t* ev = timing ? &r->stageEv[k * 10] : nullptr;
             if (timing) CK(cudaEventRecord(ev[0], st));
             launch_control(r->q, st);
             if (timing) CK(cudaEventRecord(ev[1], st));
@@ -522,7 +522,7 @@ static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, con
             if (timing) CK(cudaEventRecord(ev[2], st));
             launch_trace_extension(s->view, r->q, r->soa, f, traceGrid, st);
             if (timing) CK(cudaEventRecord(ev[3], st));
-            launch_trace_shadow(s->view, r->q, r->soa, traceGrid, st);
+            launch_trace_shadow(s->view, r->q, r->soa, f, traceGrid, st);
             if (timing) CK(cudaEventRecord(ev[4], st));
             for (uint32_t b = 0; b < kNumBuckets; ++b) {
                 launch_shade_bucket(b, s->view, r->q, r->soa, f, shadeGrid, st);
@@ -537,7 +537,7 @@ static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, con
             for (uint32_t k = 0; k < kChunk; ++k)
                 for (int j = 0; j < WRK_NUM_STAGES; ++j) {
                     float ms = 0;
-                    CK(cudaEventElapsedTime(&ms, r->stageEv[k * 9 + j], r->stageEv[k * 9 + j + 1]));
+                    CK(cudaEventElapsedTime(&ms, r->stageEv[k * 10 + j], r->stageEv[k * 10 + j + 1]));
                     stageMs[j] += ms;
                     stageN[j] += 1;
                 }
@@ -545,7 +545,7 @@ static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, con
         const Counters& h = *r->hostCtr;
         uint32_t out = h.cur ^ 1u;
         if (h.error) return fail(WRK_ERR_DEVICE, "device error flags 0x%x during render", h.error);
-        if (h.nextWork == h.totalWork && h.ext[out] == 0 && h.shd[out] == 0) break;
+        if (h.nextWork == h.totalWork && h.ext[out].v == 0 && h.shd[out].v == 0) break;
         if (iters > maxIters) return fail(WRK_ERR_DEVICE, "render did not converge after %u iterations", iters);
     }
     CK(cudaEventRecord(r->evLoop1, st));
@@ -556,8 +556,10 @@ static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, con
     if (stats) {
         const Counters& h = *r->hostCtr;
         stats->paths = h.paths;
+        // the last iteration's queues were never folded in by a following control step
         stats->extensionRays = h.extRays;
         stats->shadowRays = h.shdRays;
+        for (int b = 0; b < kNumBuckets; ++b) stats->bucketPaths[b] = h.bucketTotal[b] + h.bucket[b].v;
         stats->iterations = iters;
         stats->deviceErrors = h.error;
         cudaEventElapsedTime(&stats->gpuMs, r->evLoop0, r->evLoop1);

@@ -42,26 +42,33 @@ __device__ __forceinline__ void warp_append_r(uint32_t* q, uint32_t* counter, bo
 
 __global__ void k_control(Queues q) {
     Counters* c = q.ctr;
+    // statistics of the iteration that just finished
+    for (int b = 0; b < kNumBuckets; ++b) c->bucketTotal[b] += c->bucket[b].v;
     uint32_t cur = c->cur ^ 1u;
     uint32_t out = cur ^ 1u;
     c->cur = cur;
-    c->ext[out] = 0;
-    c->shd[out] = 0;
-    for (int b = 0; b < kNumBuckets; ++b) c->bucket[b] = 0;
+    c->ext[out].v = 0;
+    c->shd[out].v = 0;
+    for (int b = 0; b < kNumBuckets; ++b) c->bucket[b].v = 0;
+    c->fetchExtension.v = 0;
+    c->fetchShadow.v = 0;
     unsigned long long remaining = c->totalWork - c->nextWork;
-    if (c->freeCount > q.capacity || c->ext[cur] > q.capacity) {
+    if (c->freeCount.v > q.capacity || c->ext[cur].v > q.capacity || c->shd[cur].v > q.capacity) {
         c->error |= kErrQueueOverflow;
-        c->freeCount = 0;
+        c->freeCount.v = 0;
     }
-    uint32_t g = (uint32_t)min((unsigned long long)c->freeCount, remaining);
-    g = min(g, q.capacity - c->ext[cur]);
+    uint32_t g = (uint32_t)min((unsigned long long)c->freeCount.v, remaining);
+    g = min(g, q.capacity - min(c->ext[cur].v, q.capacity));
     c->genCount = g;
-    c->genFreeBase = c->freeCount - g;
-    c->freeCount -= g;
+    c->genFreeBase = c->freeCount.v - g;
+    c->freeCount.v -= g;
     c->genWorkBase = c->nextWork;
     c->nextWork += g;
-    c->genExtBase = c->ext[cur];
-    c->ext[cur] += g;
+    c->genExtBase = c->ext[cur].v;
+    c->ext[cur].v += g;
+    c->paths += g;
+    c->extRays += c->ext[cur].v;
+    c->shdRays += c->shd[cur].v;
     c->iteration += 1;
 }
 
@@ -74,7 +81,6 @@ __global__ void __launch_bounds__(kShadeBlock) k_generate(Queues q, PathSoA p, F
     const uint32_t cur = c->cur;
     const uint32_t fb = c->genFreeBase, eb = c->genExtBase;
     const unsigned long long wb = c->genWorkBase;
-    uint32_t made = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g; i += gridDim.x * blockDim.x) {
         uint32_t slot = q.freeStack[fb + i];
         unsigned long long w = wb + i;
@@ -117,9 +123,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_generate(Queues q, PathSoA p, F
         p.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(pixel));
         p.st[slot] = make_uint4(seed, 0u, 0u, kFlagFirstHit | kFlagPrevDelta);
         q.ext[cur][eb + i] = slot;
-        ++made;
     }
-    if (made) atomicAdd(&c->paths, (unsigned long long)made);
 }
 
 void launch_generate(const Queues& q, const PathSoA& p, const Frame& f, int grid, cudaStream_t st) {
@@ -330,12 +334,13 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathSoA& p, co
     const wrk_material m = s.mats[mat];
     if (m.normalTextureId > 0) h.n = normal_mapped(s, m, h);
     if (kBucket == kBucketLambert) {
+        // getMaterialAlbedo is a pure function of (material, uv): fetch it once
+        const float3 al = albedo_of(s, m, h.u, h.v);
         if (f.useNEE && s.numEmissive > 0 && !(r.flags & kFlagNeeDone)) {
             LightSample ls;
             if (sample_light(s, r, h, ls)) {
                 float bpdf = cosine_pdf(ls.cosTheta);
                 float w = power_heuristic(ls.lpdf, bpdf);
-                float3 al = albedo_of(s, m, h.u, h.v);
                 float3 fb = f3(al.x / kPi * ls.cosTheta, al.y / kPi * ls.cosTheta, al.z / kPi * ls.cosTheta);
                 float3 con = f3(r.thr.x * fb.x * ls.le.x * w / ls.lpdf, r.thr.y * fb.y * ls.le.y * w / ls.lpdf,
                                 r.thr.z * fb.z * ls.le.z * w / ls.lpdf);
@@ -358,7 +363,6 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathSoA& p, co
             float pdf;
             float3 loc = cosine_hemisphere(u1, u2, pdf);
             float3 wd = to_world(loc, h.n, tg, bt);
-            float3 al = albedo_of(s, m, h.u, h.v);
             r.thr = mul(r.thr, al);
             r.prevPdf = pdf;
             r.flags &= ~kFlagPrevDelta;
@@ -453,7 +457,7 @@ template <uint32_t kBucket>
 __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, Queues q, PathSoA p, Frame f) {
     Counters* c = q.ctr;
     const uint32_t cur = c->cur, nxt = cur ^ 1u;
-    const uint32_t n = min(c->bucket[kBucket], q.capacity);
+    const uint32_t n = min(c->bucket[kBucket].v, q.capacity);
     const uint32_t* in = q.bucket[kBucket];
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         uint32_t i = base + threadIdx.x;
@@ -462,10 +466,11 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, Queues q, Pat
             atomicOr(&c->error, kErrBadIndex);
             slot = kInvalidSlot;
         }
-        int out = slot != kInvalidSlot ? shade_one<kBucket>(s, p, f, slot) : kOutNone;
-        warp_append_r(q.ext[nxt], &c->ext[nxt], out == kOutExt, slot, q.capacity, &c->error);
-        warp_append_r(q.shd[nxt], &c->shd[nxt], out == kOutShadow, slot, q.capacity, &c->error);
-        warp_append_r(q.freeStack, &c->freeCount, out == kOutFree, slot, q.capacity, &c->error);
+        constexpr uint32_t kCode = kBucket == kBucketLambertResume ? kBucketLambert : kBucket;
+        int out = slot != kInvalidSlot ? shade_one<kCode>(s, p, f, slot) : kOutNone;
+        warp_append_r(q.ext[nxt], &c->ext[nxt].v, out == kOutExt, slot, q.capacity, &c->error);
+        warp_append_r(q.shd[nxt], &c->shd[nxt].v, out == kOutShadow, slot, q.capacity, &c->error);
+        warp_append_r(q.freeStack, &c->freeCount.v, out == kOutFree, slot, q.capacity, &c->error);
     }
 }
 
@@ -475,6 +480,7 @@ void launch_shade_bucket(uint32_t b, const DevScene& s, const Queues& q, const P
         case kBucketLambert: k_shade<kBucketLambert><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
         case kBucketDielectric: k_shade<kBucketDielectric><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
         case kBucketGGX: k_shade<kBucketGGX><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
+        case kBucketLambertResume: k_shade<kBucketLambertResume><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
         default: k_shade<kBucketOther><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
     }
 }
@@ -484,6 +490,7 @@ void launch_shade(const DevScene& s, const Queues& q, const PathSoA& p, const Fr
     k_shade<kBucketDielectric><<<grid, kShadeBlock, 0, st>>>(s, q, p, f);
     k_shade<kBucketGGX><<<grid, kShadeBlock, 0, st>>>(s, q, p, f);
     k_shade<kBucketOther><<<grid, kShadeBlock, 0, st>>>(s, q, p, f);
+    k_shade<kBucketLambertResume><<<grid, kShadeBlock, 0, st>>>(s, q, p, f);
 }
 
 // rgb = sum * (1/spp) as renderer.cpp:308-313; guides averaged unless raw.

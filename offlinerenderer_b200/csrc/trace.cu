@@ -101,81 +101,119 @@ __device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, 
     }
 }
 
-// Closest hit with ties broken toward the lower primitive index.  Returns false
-// on miss.  *err gets kErrStackOverflow if the stack limit is reached.
+// Per-lane traversal state, kept in registers across the persistent loop's rounds.
+struct Trav {
+    Ray r;
+    float ix, iy, iz;
+    uint32_t octInv;
+    uint32_t gBase, gHits, gImask, tBase, tMask;
+    int sp;
+    uint32_t visits;
+    float tBest;
+    uint32_t pBest, mBest;
+};
+
+__device__ __forceinline__ void trav_init(Trav& t, const Ray& r) {
+    t.r = r;
+    t.ix = 1.0f / r.dx;
+    t.iy = 1.0f / r.dy;
+    t.iz = 1.0f / r.dz;
+    uint32_t oct = (r.dx < 0.0f ? 1u : 0u) | (r.dy < 0.0f ? 2u : 0u) | (r.dz < 0.0f ? 4u : 0u);
+    t.octInv = oct ^ 7u;  // slot of the child nearest the entry corner -> bit 0
+    // the root is a one-child node group
+    t.gBase = 0;
+    t.gHits = 1u << t.octInv;
+    t.gImask = 1u;
+    t.tBase = 0;
+    t.tMask = 0;
+    t.sp = 0;
+    t.visits = 0;
+    t.tBest = r.tmax;
+    t.pBest = kNoHit;
+    t.mBest = 0;
+}
+
+// One traversal step: descend into the next child of the current node group
+// (pushing the group's remainder), test the triangles that node exposes, and pop
+// when the group is used up.  Returns true when the ray is finished.  Closest hit
+// keeps ties in t with the lower primitive index; any hit stops at the first hit.
+template <bool kAnyHit>
+__device__ __forceinline__ bool trav_step(const DevScene& s, Trav& t, uint2* sstack, uint2* lstack,
+                                          uint32_t* errFlag) {
+    const int tid = threadIdx.x;
+    if (++t.visits > kMaxVisits) {  // a malformed tree must not spin forever
+        atomicOr(errFlag, kErrBadIndex);
+        return true;
+    }
+    if (t.gHits) {
+        uint32_t pos = __ffs(t.gHits) - 1;
+        t.gHits &= t.gHits - 1;
+        uint32_t slot = pos ^ t.octInv;
+        uint32_t child = t.gBase + __popc(t.gImask & ((1u << slot) - 1u));
+        if (t.gHits) {
+            uint2 e = make_uint2(t.gBase, t.gHits | (t.gImask << 8));
+            if (t.sp < kStackSmem) sstack[t.sp * kTraceBlock + tid] = e;
+            else if (t.sp < kStackSmem + kStackLocal) lstack[t.sp - kStackSmem] = e;
+            else {
+                atomicOr(errFlag, kErrStackOverflow);
+                return true;
+            }
+            ++t.sp;
+        }
+        if (child >= s.numNodes) {
+            atomicOr(errFlag, kErrBadIndex);
+            return true;
+        }
+        intersect_node(s.nodes, child, t.r, t.ix, t.iy, t.iz, t.octInv, t.tBest, t.gBase, t.tBase, t.gHits, t.gImask,
+                       t.tMask);
+        if (t.tMask && t.tBase + (31u - __clz(t.tMask)) >= s.numTris) {
+            atomicOr(errFlag, kErrBadIndex);
+            return true;
+        }
+    }
+    while (t.tMask) {
+        uint32_t j = __ffs(t.tMask) - 1;
+        t.tMask &= t.tMask - 1;
+        const float4* tp = s.tris + 3 * (size_t)(t.tBase + j);
+        float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+        float th;
+        if (mt_rn(t.r, a, b, c, th) && th >= t.r.tmin && th <= t.r.tmax) {
+            uint32_t prim = __float_as_uint(a.w);
+            if (kAnyHit) {
+                t.tBest = th;
+                t.pBest = prim;
+                return true;
+            }
+            if (th < t.tBest || (th == t.tBest && prim < t.pBest)) {
+                t.tBest = th;
+                t.pBest = prim;
+                t.mBest = __float_as_uint(b.w);
+            }
+        }
+    }
+    if (!t.gHits) {
+        if (t.sp == 0) return true;
+        --t.sp;
+        uint2 e = t.sp < kStackSmem ? sstack[t.sp * kTraceBlock + tid] : lstack[t.sp - kStackSmem];
+        t.gBase = e.x;
+        t.gHits = e.y & 0xffu;
+        t.gImask = e.y >> 8;
+    }
+    return false;
+}
+
 template <bool kAnyHit>
 __device__ __forceinline__ bool traverse(const DevScene& s, const Ray& r, float& tBest, uint32_t& pBest,
                                          uint32_t& mBest, uint2* sstack, uint32_t* errFlag) {
-    float ix = 1.0f / r.dx, iy = 1.0f / r.dy, iz = 1.0f / r.dz;
-    uint32_t oct = (r.dx < 0.0f ? 1u : 0u) | (r.dy < 0.0f ? 2u : 0u) | (r.dz < 0.0f ? 4u : 0u);
-    uint32_t oct_inv = oct ^ 7u;  // slot of the child nearest the entry corner -> bit 0
-    tBest = r.tmax;
-    pBest = kNoHit;
-    mBest = 0;
     uint2 lstack[kStackLocal];
-    int sp = 0;
-    // node group: (base, hits, imask); the root is a one-child group
-    uint32_t gBase = 0, gHits = 1u << (0u ^ oct_inv), gImask = 1u;
-    uint32_t tBase = 0, tMask = 0;
-    const int tid = threadIdx.x;
-    uint32_t visits = 0;
-    while (true) {
-        if (++visits > kMaxVisits) {  // a malformed tree must not spin forever
-            atomicOr(errFlag, kErrBadIndex);
-            return pBest != kNoHit;
-        }
-        if (gHits) {
-            uint32_t pos = __ffs(gHits) - 1;
-            gHits &= gHits - 1;
-            uint32_t slot = pos ^ oct_inv;
-            uint32_t child = gBase + __popc(gImask & ((1u << slot) - 1u));
-            if (gHits) {
-                uint2 e = make_uint2(gBase, gHits | (gImask << 8));
-                if (sp < kStackSmem) sstack[sp * kTraceBlock + tid] = e;
-                else if (sp < kStackSmem + kStackLocal) lstack[sp - kStackSmem] = e;
-                else { atomicOr(errFlag, kErrStackOverflow); return pBest != kNoHit; }
-                ++sp;
-            }
-            if (child >= s.numNodes) {
-                atomicOr(errFlag, kErrBadIndex);
-                return pBest != kNoHit;
-            }
-            intersect_node(s.nodes, child, r, ix, iy, iz, oct_inv, tBest, gBase, tBase, gHits, gImask, tMask);
-            if (tMask && tBase + (31u - __clz(tMask)) >= s.numTris) {
-                atomicOr(errFlag, kErrBadIndex);
-                return pBest != kNoHit;
-            }
-        }
-        while (tMask) {
-            uint32_t j = __ffs(tMask) - 1;
-            tMask &= tMask - 1;
-            const float4* tp = s.tris + 3 * (size_t)(tBase + j);
-            float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-            float t;
-            if (mt_rn(r, a, b, c, t) && t >= r.tmin && t <= r.tmax) {
-                uint32_t prim = __float_as_uint(a.w);
-                if (kAnyHit) {
-                    tBest = t;
-                    pBest = prim;
-                    return true;
-                }
-                if (t < tBest || (t == tBest && prim < pBest)) {
-                    tBest = t;
-                    pBest = prim;
-                    mBest = __float_as_uint(b.w);
-                }
-            }
-        }
-        if (!gHits) {
-            if (sp == 0) break;
-            --sp;
-            uint2 e = sp < kStackSmem ? sstack[sp * kTraceBlock + tid] : lstack[sp - kStackSmem];
-            gBase = e.x;
-            gHits = e.y & 0xffu;
-            gImask = e.y >> 8;
-        }
+    Trav t;
+    trav_init(t, r);
+    while (!trav_step<kAnyHit>(s, t, sstack, lstack, errFlag)) {
     }
-    return pBest != kNoHit;
+    tBest = t.tBest;
+    pBest = t.pBest;
+    mBest = t.mBest;
+    return t.pBest != kNoHit;
 }
 
 __device__ __forceinline__ Ray load_ray8(const float* p) {
@@ -237,10 +275,6 @@ __device__ __forceinline__ void warp_append(uint32_t* q, uint32_t* counter, bool
         else atomicOr(err, kErrQueueOverflow);
     }
 }
-__device__ __forceinline__ void warp_count64(unsigned long long* counter, bool pred) {
-    uint32_t b = __ballot_sync(0xffffffffu, pred);
-    if (b && (threadIdx.x & 31u) == (uint32_t)(__ffs(b) - 1)) atomicAdd(counter, (unsigned long long)__popc(b));
-}
 
 __device__ __forceinline__ uint32_t bucket_of(uint32_t type) {
     switch (type) {
@@ -252,84 +286,106 @@ __device__ __forceinline__ uint32_t bucket_of(uint32_t type) {
     }
 }
 
-__global__ void __launch_bounds__(kTraceBlock) k_trace_extension(DevScene s, Queues q, PathSoA p, Frame f) {
+// Persistent traversal: each warp keeps its lanes busy by fetching new rays from
+// the queue (one warp-aggregated atomic on a per-launch fetch counter) whenever
+// fewer than kRefillAt lanes still have a ray in flight, instead of waiting for
+// the slowest ray of a fixed batch (Aila & Laine 2009, "Understanding the
+// efficiency of ray traversal on GPUs").  Finished lanes hand their results on
+// with warp-aggregated queue appends.
+#ifndef WRK_REFILL_AT
+#define WRK_REFILL_AT 16
+#endif
+#ifndef WRK_TRACE_MIN_BLOCKS
+#define WRK_TRACE_MIN_BLOCKS 8
+#endif
+constexpr int kRefillAt = WRK_REFILL_AT;
+
+template <bool kAnyHit>
+__global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_persistent(DevScene s, Queues q,
+                                                                                      PathSoA p, Frame f) {
     __shared__ uint2 sstack[kStackSmem * kTraceBlock];
+    uint2 lstack[kStackLocal];
     Counters* c = q.ctr;
     const uint32_t cur = c->cur;
-    const uint32_t n = min(c->ext[cur], q.capacity);
-    const uint32_t* in = q.ext[cur];
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        uint32_t i = base + threadIdx.x;
-        uint32_t slot = i < n ? in[i] : kInvalidSlot;
-        if (slot != kInvalidSlot && slot >= q.capacity) {
-            atomicOr(&c->error, kErrBadIndex);
-            slot = kInvalidSlot;
-        }
-        bool valid = slot != kInvalidSlot;
-        bool hit = false, miss = false;
-        uint32_t bucket = kNumBuckets;
-        if (valid) {
-            float4 o = p.ray_o[slot], d = p.ray_d[slot];
-            Ray r{o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w};
-            float t;
-            uint32_t prim, mat;
-            hit = traverse<false>(s, r, t, prim, mat, sstack, &c->error);
-            if (hit) {
-                p.hit[slot] = make_float4(t, __uint_as_float(prim), __uint_as_float(mat), 0.0f);
-                bucket = mat < s.numMats ? bucket_of(s.mats[mat].type) : kBucketOther;
-            } else {
-                // __miss__trace + raygen miss branch (trace.cu:143-148): add T*env, accumulate, terminate
-                miss = true;
-                float4 th = p.thr[slot], rd = p.rad[slot];
-                float3 L = make_float3(rd.x + th.x * s.env[0], rd.y + th.y * s.env[1], rd.z + th.z * s.env[2]);
-                L = clamp_fireflies(L, f.fireflyClamp);
-                atomicAdd(f.accum + __float_as_uint(rd.w), make_float4(L.x, L.y, L.z, 0.0f));
+    const uint32_t n = min(kAnyHit ? c->shd[cur].v : c->ext[cur].v, q.capacity);
+    const uint32_t* in = kAnyHit ? q.shd[cur] : q.ext[cur];
+    uint32_t* fetch = kAnyHit ? &c->fetchShadow.v : &c->fetchExtension.v;
+    const uint32_t lane = threadIdx.x & 31u;
+    Trav t;
+    uint32_t slot = kInvalidSlot;
+    bool active = false, exhausted = false;
+    while (true) {
+        uint32_t idle = __ballot_sync(0xffffffffu, !active && !exhausted);
+        if (idle) {
+            uint32_t leader = __ffs(idle) - 1, base = 0;
+            if (lane == leader) base = atomicAdd(fetch, (uint32_t)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (!active && !exhausted) {
+                uint32_t idx = base + __popc(idle & ((1u << lane) - 1u));
+                if (idx < n) {
+                    slot = in[idx];
+                    if (slot < q.capacity) {
+                        float4 o = kAnyHit ? p.sh_o[slot] : p.ray_o[slot];
+                        float4 d = kAnyHit ? p.sh_d[slot] : p.ray_d[slot];
+                        trav_init(t, Ray{o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w});
+                        active = true;
+                    } else {
+                        atomicOr(&c->error, kErrBadIndex);
+                    }
+                } else {
+                    exhausted = true;
+                }
             }
         }
-        warp_count64(&c->extRays, valid);
-#pragma unroll
-        for (uint32_t b = 0; b < kNumBuckets; ++b)
-            warp_append(q.bucket[b], &c->bucket[b], bucket == b, slot, q.capacity, &c->error);
-        warp_append(q.freeStack, &c->freeCount, miss, slot, q.capacity, &c->error);
-    }
-}
-
-__global__ void __launch_bounds__(kTraceBlock) k_trace_shadow(DevScene s, Queues q, PathSoA p) {
-    __shared__ uint2 sstack[kStackSmem * kTraceBlock];
-    Counters* c = q.ctr;
-    const uint32_t cur = c->cur;
-    const uint32_t n = min(c->shd[cur], q.capacity);
-    const uint32_t* in = q.shd[cur];
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        uint32_t i = base + threadIdx.x;
-        uint32_t slot = i < n ? in[i] : kInvalidSlot;
-        if (slot != kInvalidSlot && slot >= q.capacity) {
-            atomicOr(&c->error, kErrBadIndex);
-            slot = kInvalidSlot;
-        }
-        bool valid = slot != kInvalidSlot;
-        if (valid) {
-            float4 o = p.sh_o[slot], d = p.sh_d[slot];
-            Ray r{o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w};
-            float t;
-            uint32_t prim, mat;
-            // Shadow stage of __raygen__trace (trace.cu:27-51): add the NEE contribution if unoccluded.
-            if (!traverse<true>(s, r, t, prim, mat, sstack, &c->error)) {
+        if (__all_sync(0xffffffffu, exhausted && !active)) break;
+        // once the queue is drained nothing can refill a lane: run to completion
+        const int refillAt = __any_sync(0xffffffffu, exhausted) ? 1 : kRefillAt;
+        bool fin = false;
+        do {
+            if (active && !fin) fin = trav_step<kAnyHit>(s, t, sstack, lstack, &c->error);
+        } while (__popc(__ballot_sync(0xffffffffu, active && !fin)) >= refillAt);
+        const bool done = active && fin;
+        if (kAnyHit) {
+            // Shadow stage of __raygen__trace (trace.cu:27-51): add the NEE
+            // contribution if nothing lies in [tmin, tmax], then resume shading.
+            if (done && t.pBest == kNoHit) {
                 float4 rd = p.rad[slot], cc = p.sh_c[slot];
                 p.rad[slot] = make_float4(rd.x + cc.x, rd.y + cc.y, rd.z + cc.z, rd.w);
             }
+            warp_append(q.bucket[kBucketLambertResume], &c->bucket[kBucketLambertResume].v, done, slot, q.capacity,
+                        &c->error);
+        } else {
+            uint32_t bucket = kNumBuckets;
+            bool miss = false;
+            if (done) {
+                if (t.pBest != kNoHit) {
+                    p.hit[slot] = make_float4(t.tBest, __uint_as_float(t.pBest), __uint_as_float(t.mBest), 0.0f);
+                    bucket = t.mBest < s.numMats ? bucket_of(s.mats[t.mBest].type) : kBucketOther;
+                } else {
+                    // __miss__trace + the raygen miss branch (trace.cu:143-148)
+                    miss = true;
+                    float4 th = p.thr[slot], rd = p.rad[slot];
+                    float3 L = make_float3(rd.x + th.x * s.env[0], rd.y + th.y * s.env[1], rd.z + th.z * s.env[2]);
+                    L = clamp_fireflies(L, f.fireflyClamp);
+                    atomicAdd(f.accum + __float_as_uint(rd.w), make_float4(L.x, L.y, L.z, 0.0f));
+                }
+            }
+#pragma unroll
+            for (uint32_t b = 0; b < kBucketLambertResume; ++b)
+                warp_append(q.bucket[b], &c->bucket[b].v, bucket == b, slot, q.capacity, &c->error);
+            warp_append(q.freeStack, &c->freeCount.v, miss, slot, q.capacity, &c->error);
         }
-        warp_count64(&c->shdRays, valid);
-        warp_append(q.bucket[kBucketLambert], &c->bucket[kBucketLambert], valid, slot, q.capacity, &c->error);
+        if (done) active = false;
     }
 }
 
 void launch_trace_extension(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid,
                             cudaStream_t st) {
-    k_trace_extension<<<grid, kTraceBlock, 0, st>>>(s, q, p, f);
+    k_trace_persistent<false><<<grid, kTraceBlock, 0, st>>>(s, q, p, f);
 }
-void launch_trace_shadow(const DevScene& s, const Queues& q, const PathSoA& p, int grid, cudaStream_t st) {
-    k_trace_shadow<<<grid, kTraceBlock, 0, st>>>(s, q, p);
+void launch_trace_shadow(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid,
+                         cudaStream_t st) {
+    k_trace_persistent<true><<<grid, kTraceBlock, 0, st>>>(s, q, p, f);
 }
 
 }  // namespace wrk

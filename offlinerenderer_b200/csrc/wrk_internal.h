@@ -23,7 +23,16 @@ namespace wrk {
 
 enum : uint32_t { kLambert = 0, kEmissive = 1, kGlass = 2, kGGX = 3, kGGXT = 4 };
 // Material buckets the trace kernel sorts hits into.
-enum : uint32_t { kBucketLambert = 0, kBucketDielectric = 1, kBucketGGX = 2, kBucketOther = 3, kNumBuckets = 4 };
+// Lambert hits that still owe their NEE light sample and Lambert paths resuming
+// after their shadow ray take separate buckets so each warp runs one branch.
+enum : uint32_t {
+    kBucketLambert = 0,
+    kBucketDielectric = 1,
+    kBucketGGX = 2,
+    kBucketOther = 3,
+    kBucketLambertResume = 4,
+    kNumBuckets = 5
+};
 // st.w flags
 enum : uint32_t { kFlagFirstHit = 1u, kFlagPrevDelta = 2u, kFlagNeeDone = 4u };
 
@@ -71,25 +80,38 @@ struct PathSoA {
     float4* sh_c;
 };
 
+// A queue counter alone on a 128-byte line, so appends to different queues hit
+// different L2 lines instead of serializing on one.
+struct alignas(128) HotCounter {
+    uint32_t v;
+    uint32_t pad[31];
+};
+
 // Queue counters and loop bookkeeping; lives in device memory, owned by the renderer.
+// The hot counters take warp-aggregated atomics; everything after them is written
+// only by the single-thread control kernel (which also keeps the statistics, so
+// no kernel spends atomics on them).
 struct Counters {
-    uint32_t ext[2];
-    uint32_t shd[2];
-    uint32_t bucket[kNumBuckets];
-    uint32_t freeCount;
-    uint32_t cur;         // which ext/shd buffer the current iteration consumes
-    uint32_t genCount;    // paths generated this iteration
-    uint32_t genFreeBase; // free-stack index of the first slot popped this iteration
-    uint32_t genExtBase;  // extension-queue index where the generated paths go
+    HotCounter ext[2];
+    HotCounter shd[2];
+    HotCounter bucket[kNumBuckets];
+    HotCounter freeCount;
+    HotCounter fetchExtension;  // rays taken by the persistent traversal kernels this iteration
+    HotCounter fetchShadow;
+    uint32_t cur;          // which ext/shd buffer the current iteration consumes
+    uint32_t genCount;     // paths generated this iteration
+    uint32_t genFreeBase;  // free-stack index of the first slot popped this iteration
+    uint32_t genExtBase;   // extension-queue index where the generated paths go
     uint32_t iteration;
+    uint32_t error;
+    uint32_t pad[2];
     unsigned long long nextWork;
     unsigned long long totalWork;
     unsigned long long genWorkBase;
     unsigned long long extRays;
     unsigned long long shdRays;
     unsigned long long paths;
-    uint32_t error;
-    uint32_t pad;
+    unsigned long long bucketTotal[kNumBuckets];
 };
 
 struct Queues {
@@ -119,7 +141,8 @@ void launch_control(const Queues& q, cudaStream_t st);
 void launch_generate(const Queues& q, const PathSoA& p, const Frame& f, int grid, cudaStream_t st);
 void launch_trace_extension(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid,
                             cudaStream_t st);
-void launch_trace_shadow(const DevScene& s, const Queues& q, const PathSoA& p, int grid, cudaStream_t st);
+void launch_trace_shadow(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid,
+                         cudaStream_t st);
 void launch_shade(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid, cudaStream_t st);
 void launch_shade_bucket(uint32_t bucket, const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f,
                          int grid, cudaStream_t st);

@@ -23,7 +23,8 @@ LIB_PATH = os.path.join(HERE, "libwrk.so")
 WRK_FLAG_RAW_GUIDES = 1
 WRK_FLAG_STAGE_TIMING = 2
 STAGES = ["control", "generate", "trace_extension", "trace_shadow", "shade_lambert", "shade_dielectric", "shade_ggx",
-          "shade_emissive"]
+          "shade_emissive", "shade_lambert_resume"]
+BUCKETS = ["lambert", "dielectric", "ggx", "other", "lambert_resume"]
 
 
 class WrkError(RuntimeError):
@@ -53,7 +54,8 @@ class RenderParamsC(C.Structure):
 class RenderStatsC(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("extensionRays", C.c_uint64), ("shadowRays", C.c_uint64),
                 ("iterations", C.c_uint32), ("deviceErrors", C.c_uint32), ("gpuMs", C.c_float),
-                ("totalMs", C.c_float), ("stageMs", C.c_float * 8), ("stageLaunches", C.c_uint32 * 8)]
+                ("totalMs", C.c_float), ("stageMs", C.c_float * 9), ("stageLaunches", C.c_uint32 * 9),
+                ("bucketPaths", C.c_uint64 * 5)]
 
 
 class BvhInfoC(C.Structure):
@@ -187,7 +189,8 @@ def params_struct(st, spp=None, max_iterations=8, raw_guides=False, seed=None, s
 
 
 def _stats_dict(stats: "RenderStatsC") -> dict:
-    d = {k: getattr(stats, k) for k, _ in RenderStatsC._fields_ if k not in ("stageMs", "stageLaunches")}
+    d = {k: getattr(stats, k) for k, _ in RenderStatsC._fields_ if k not in ("stageMs", "stageLaunches", "bucketPaths")}
+    d["bucketPaths"] = {n: stats.bucketPaths[i] for i, n in enumerate(BUCKETS)}
     d["stageMs"] = {n: stats.stageMs[i] for i, n in enumerate(STAGES)}
     d["stageLaunches"] = {n: stats.stageLaunches[i] for i, n in enumerate(STAGES)}
     return d

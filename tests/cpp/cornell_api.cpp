@@ -5,6 +5,7 @@
 #include <wr/wr.h>
 
 #include <cstdio>
+#include <stdexcept>
 #include <vector>
 
 int main(int argc, char** argv) {
