@@ -171,6 +171,16 @@ int wrk_trace_occluded(wrk_scene* s, const float* d_rays, uint32_t n, uint32_t* 
 /* Stable compaction (compact.cu:6-17): keeps idxIn[i] whose stage[idxIn[i]] != 3,
  * in input order; *d_count receives the survivor count. */
 int wrk_compact(const uint32_t* d_stage, const uint32_t* d_idxIn, uint32_t n, uint32_t* d_idxOut, uint32_t* d_count);
+/* wrk_compact without any allocation -- no counterpart in the reference (its
+ * compact kernel is handed buffers the renderer allocated).  For callers that may
+ * not allocate device memory (a fixed, pre-reserved memory budget; an allocator
+ * that must own all device memory): the per-tile counts live in a 256 KiB array
+ * built into the library, so n is limited to 67,108,864 indices (larger n returns
+ * WRK_ERR_INVALID).  The first call on a device resolves that array's address and
+ * should come before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialized by the caller. */
+int wrk_compact_noalloc(const uint32_t* d_stage, const uint32_t* d_idxIn, uint32_t n, uint32_t* d_idxOut,
+                        uint32_t* d_count);
 /* Light selection (sampleEmissiveTriangle, sampling.cuh:116-135). */
 int wrk_cdf_sample(const float* d_cdf, uint32_t ncdf, const float* d_u, uint32_t n, uint32_t* d_out);
 /* PCG hash with dimension and its uniform (sampling.cuh:24-38). */

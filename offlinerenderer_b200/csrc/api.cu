@@ -107,6 +107,11 @@ void camera_frame(const wrk_camera& c, Frame& f) {
 
 }  // namespace
 
+namespace wrk {
+// Records a failure for wrk_last_error() from entry points defined in other files.
+int report_error(int code, const char* msg) { return fail(code, "%s", msg); }
+}  // namespace wrk
+
 struct wrk_scene {
     int device = 0;
     std::vector<float> vtx, nrm, uv;

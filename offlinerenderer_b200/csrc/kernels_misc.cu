@@ -2,6 +2,8 @@
 // ballot/prefix-sum compaction, light-CDF selection, RNG, the BSDF math batch,
 // texture fetch, camera rays, and the ACES tonemap.  These are the same device
 // functions the renderer uses, exposed one at a time for parity checks.
+#include <mutex>
+
 #include "wrk_internal.h"
 #include "wrk_shading.cuh"
 
@@ -224,3 +226,82 @@ void launch_tonemap(const float* rgb, uint32_t nfloat, uint8_t* out, int grid, i
 }
 
 }  // namespace wrk
+
+// ---------------------------------------------------------------------------
+// Compaction for callers that cannot allocate device memory.
+//
+// wrk_compact obtains its per-tile count buffer with cudaMallocAsync.  Some
+// callers cannot let a library allocate: a serving process that reserved its
+// whole device-memory budget up front and must not grow, a framework whose own
+// allocator has to own every device byte, and hosts that forbid allocation after
+// start-up so that memory use stays fixed.  For them wrk_compact_noalloc keeps
+// that scratch in a fixed array that is part of the library image itself (loaded
+// with the module, resident on every GPU that loads the library until the
+// process exits), so the call allocates nothing.
+//
+// The first call on each device resolves the array's device address (with
+// cudaGetSymbolAddress, that device current); make that first call before any
+// stream capture begins.
+//
+// Limit: at most kNoAllocMaxTiles tiles of 1024 entries (67,108,864 input
+// indices), i.e. 256 KiB of scratch per GPU.  Every call shares this one array
+// and it keeps the previous call's values; each call writes every tile count it
+// reads before reading it, so nothing has to be cleared first.  Calls that overlap
+// on the GPU (other host threads, other streams) race on the array and must be
+// serialized by the caller.
+namespace wrk {
+namespace {
+
+constexpr uint32_t kNoAllocMaxTiles = 65536;
+static __device__ __align__(256) uint32_t g_compactScratch[kNoAllocMaxTiles];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratchMutex;
+uint32_t* g_scratchAddr[kMaxDevices] = {nullptr};
+
+// The array's name in host code is only a host-side handle of the device symbol,
+// not a device address: resolve the device address once per device, with that
+// device current, and pass the pointer to the kernels.
+int scratch_for_current_device(uint32_t** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return report_error(WRK_ERR_CUDA, cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return report_error(WRK_ERR_INVALID, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_scratchMutex);
+    if (!g_scratchAddr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_compactScratch);
+        if (e != cudaSuccess) return report_error(WRK_ERR_CUDA, cudaGetErrorString(e));
+        g_scratchAddr[dev] = static_cast<uint32_t*>(p);
+    }
+    *out = g_scratchAddr[dev];
+    return WRK_OK;
+}
+
+}  // namespace
+}  // namespace wrk
+
+extern "C" int wrk_compact_noalloc(const uint32_t* d_stage, const uint32_t* d_idxIn, uint32_t n, uint32_t* d_idxOut,
+                                   uint32_t* d_count) {
+    using namespace wrk;
+    if (!d_count || (n && (!d_stage || !d_idxIn || !d_idxOut)))
+        return report_error(WRK_ERR_INVALID, "wrk_compact_noalloc: null buffer");
+    const uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
+    if (tiles > kNoAllocMaxTiles)
+        return report_error(WRK_ERR_INVALID,
+                            "wrk_compact_noalloc: n exceeds the fixed scratch limit of 67108864 indices "
+                            "(65536 tiles of 1024); use wrk_compact");
+    uint32_t* scratch = nullptr;
+    int rc = scratch_for_current_device(&scratch);
+    if (rc) return rc;
+    if (tiles == 0) {
+        cudaError_t e = cudaMemset(d_count, 0, sizeof(uint32_t));
+        return e == cudaSuccess ? WRK_OK : report_error(WRK_ERR_CUDA, cudaGetErrorString(e));
+    }
+    k_compact_count<<<tiles, kCompactTile>>>(d_stage, d_idxIn, n, scratch);
+    k_compact_scan<<<1, 1024>>>(scratch, tiles, d_count);
+    k_compact_write<<<tiles, kCompactTile>>>(d_stage, d_idxIn, n, scratch, d_idxOut);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return e == cudaSuccess ? WRK_OK : report_error(WRK_ERR_CUDA, cudaGetErrorString(e));
+}

@@ -159,6 +159,9 @@ struct BvhBuildResult {
 int build_bvh8(const float* d_vtx, const uint32_t* d_idx, const uint32_t* d_triMat, uint32_t numTris,
                cudaStream_t st, BvhBuildResult* out, char* err, size_t errlen);
 
+// Sets the per-thread message returned by wrk_last_error(); returns `code`.
+int report_error(int code, const char* msg);
+
 // standalone ray queries (trace.cu)
 void launch_closest_query(const DevScene& s, const float* rays, uint32_t n, float* t, uint32_t* prim,
                           uint32_t* err, cudaStream_t st);

@@ -93,6 +93,7 @@ SIGNATURES = {
     "wrk_trace_closest": ([_VP, _VP, _U32, _VP, _VP], _I),
     "wrk_trace_occluded": ([_VP, _VP, _U32, _VP], _I),
     "wrk_compact": ([_VP, _VP, _U32, _VP, _VP], _I),
+    "wrk_compact_noalloc": ([_VP, _VP, _U32, _VP, _VP], _I),
     "wrk_cdf_sample": ([_VP, _U32, _VP, _U32, _VP], _I),
     "wrk_rng_batch": ([_VP, _VP, _U32, _VP, _VP], _I),
     "wrk_bsdf_batch": ([_VP, _U32, _VP], _I),
