@@ -141,9 +141,8 @@ struct wrk_renderer {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evLoop0 = nullptr, evLoop1 = nullptr;
     std::vector<cudaEvent_t> stageEv;  // per-launch events for WRK_FLAG_STAGE_TIMING
-    DevBuf slots, queues, counters, frameBufs, outBufs;
+    DevBuf queues, counters, frameBufs, outBufs;
     Counters* hostCtr = nullptr;  // pinned
-    PathSoA soa{};
     Queues q{};
     ~wrk_renderer() {
         if (hostCtr) cudaFreeHost(hostCtr);
@@ -157,11 +156,6 @@ struct wrk_renderer {
 };
 
 namespace {
-
-__global__ void k_iota(uint32_t* a, uint32_t n) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) a[i] = i;
-}
 
 // Light list + power CDF exactly as Scene::finalize builds it
 // (libWR/src/internal/scene.cpp:423-491): serial FP32 over triangles in order.
@@ -430,26 +424,46 @@ int wrk_renderer_create(int device, uint32_t capacity, wrk_renderer** out) {
         return bail(fail(WRK_ERR_CUDA, "stream/event creation failed"));
     if (cudaMallocHost(&r->hostCtr, sizeof(Counters)) != cudaSuccess)
         return bail(fail(WRK_ERR_CUDA, "pinned counter allocation failed"));
+    // SoA path queues: extension x2 (5 fields), shadow x2 (9 fields), buckets (6 fields)
     size_t C = capacity;
-    if ((rc = r->slots.alloc(C * (8 * sizeof(float4) + sizeof(uint4))))) return bail(rc);
-    float4* base = r->slots.as<float4>();
-    r->soa.ray_o = base;
-    r->soa.ray_d = base + C;
-    r->soa.hit = base + 2 * C;
-    r->soa.thr = base + 3 * C;
-    r->soa.rad = base + 4 * C;
-    r->soa.sh_o = base + 5 * C;
-    r->soa.sh_d = base + 6 * C;
-    r->soa.sh_c = base + 7 * C;
-    r->soa.st = reinterpret_cast<uint4*>(base + 8 * C);
-    if ((rc = r->queues.alloc(C * sizeof(uint32_t) * (4 + kNumBuckets + 1)))) return bail(rc);
-    uint32_t* qb = r->queues.as<uint32_t>();
-    r->q.ext[0] = qb;
-    r->q.ext[1] = qb + C;
-    r->q.shd[0] = qb + 2 * C;
-    r->q.shd[1] = qb + 3 * C;
-    for (int b = 0; b < kNumBuckets; ++b) r->q.bucket[b] = qb + (4 + b) * C;
-    r->q.freeStack = qb + (4 + kNumBuckets) * C;
+    const size_t fields = 2 * 5 + 2 * 9 + kNumBuckets * 6;
+    if ((rc = r->queues.alloc(C * fields * sizeof(float4)))) return bail(rc);
+    float4* next = r->queues.as<float4>();
+    auto take = [&]() {
+        float4* p = next;
+        next += C;
+        return p;
+    };
+    for (int k = 0; k < 2; ++k) {
+        PathQ& e = r->q.ext[k];
+        e = PathQ{};
+        e.ray_o = take();
+        e.ray_d = take();
+        e.thr = take();
+        e.rad = take();
+        e.st = reinterpret_cast<uint4*>(take());
+        PathQ& h = r->q.shd[k];
+        h = PathQ{};
+        h.ray_o = take();
+        h.ray_d = take();
+        h.hit = take();
+        h.thr = take();
+        h.rad = take();
+        h.st = reinterpret_cast<uint4*>(take());
+        h.sh_o = take();
+        h.sh_d = take();
+        h.sh_c = take();
+    }
+    for (int b = 0; b < kNumBuckets; ++b) {
+        PathQ& e = r->q.bucket[b];
+        e = PathQ{};
+        e.ray_o = take();
+        e.ray_d = take();
+        e.hit = take();
+        e.thr = take();
+        e.rad = take();
+        e.st = reinterpret_cast<uint4*>(take());
+    }
     if ((rc = r->counters.alloc(sizeof(Counters)))) return bail(rc);
     r->q.ctr = r->counters.as<Counters>();
     r->q.capacity = capacity;
@@ -494,11 +508,8 @@ static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, con
     CK(cudaMemsetAsync(f.accum, 0, np * 3 * sizeof(float4), st));
     Counters c0{};
     c0.cur = 1;
-    c0.freeCount.v = r->capacity;
     c0.totalWork = (unsigned long long)np * p->spp;
     CK(cudaMemcpyAsync(r->q.ctr, &c0, sizeof(Counters), cudaMemcpyHostToDevice, st));
-    k_iota<<<(r->capacity + 255) / 256, 256, 0, st>>>(r->q.freeStack, r->capacity);
-    CK(cudaGetLastError());
     const int traceGrid = r->numSMs * 8, shadeGrid = r->numSMs * 4;
     // bound on iterations: every path needs <= maxIter; waves of `capacity` paths
     unsigned long long waves = c0.totalWork / r->capacity + 2;
@@ -523,14 +534,14 @@ static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, con
             if (timing) CK(cudaEventRecord(ev[0], st));
             launch_control(r->q, st);
             if (timing) CK(cudaEventRecord(ev[1], st));
-            launch_generate(r->q, r->soa, f, r->numSMs * 8, st);
+            launch_generate(r->q, f, r->numSMs * 8, st);
             if (timing) CK(cudaEventRecord(ev[2], st));
-            launch_trace_extension(s->view, r->q, r->soa, f, traceGrid, st);
+            launch_trace_extension(s->view, r->q, f, traceGrid, st);
             if (timing) CK(cudaEventRecord(ev[3], st));
-            launch_trace_shadow(s->view, r->q, r->soa, f, traceGrid, st);
+            launch_trace_shadow(s->view, r->q, f, traceGrid, st);
             if (timing) CK(cudaEventRecord(ev[4], st));
             for (uint32_t b = 0; b < kNumBuckets; ++b) {
-                launch_shade_bucket(b, s->view, r->q, r->soa, f, shadeGrid, st);
+                launch_shade_bucket(b, s->view, r->q, f, shadeGrid, st);
                 if (timing) CK(cudaEventRecord(ev[5 + b], st));
             }
         }

@@ -6,14 +6,17 @@
 //   libWR/kernels/shade.cu:24-85, libWR/kernels/materials/*.cuh,
 //   libWR/kernels/compact.cu:6-17.
 //
-// Paths live in SoA slots.  Each iteration:
+// A path's state travels with it through SoA queues (see wrk_internal.h).  Each
+// iteration:
 //   control   (1 thread)  swaps the extension/shadow queue buffers, clears the
-//                         material buckets, and pops free slots for new camera paths
-//   generate              camera rays for the next (sample, pixel) work items
-//   trace_extension       closest hit -> hit record + material bucket, or miss
-//   trace_shadow          any hit for pending NEE rays -> Lambert bucket (resume)
-//   shade<bucket> x4      closest-hit attributes, guides, emission, BSDF, RR;
-//                         appends to the next extension / shadow queue or frees
+//                         material buckets, and sizes the batch of new camera paths
+//                         by the room the live paths leave
+//   generate              camera rays for the next (sample, pixel) work items,
+//                         appended to the extension queue
+//   trace_extension       closest hit -> material bucket, or miss -> accumulate
+//   trace_shadow          any hit for pending NEE rays -> Lambert resume bucket
+//   shade<bucket> x5      closest-hit attributes, guides, emission, BSDF, RR;
+//                         appends to the next extension / shadow queue
 // A path carries its own iteration count; after `maxIter` iterations (8 = the
 // reference host loop's cap) a live path is dropped unaccumulated, as libWR does.
 // RNG is keyed by (pixel, sample), so the image does not depend on queue order.
@@ -24,20 +27,20 @@ namespace wrk {
 
 constexpr int kShadeBlock = 256;
 
-__device__ __forceinline__ void warp_append_r(uint32_t* q, uint32_t* counter, bool pred, uint32_t value,
-                                              uint32_t cap, uint32_t* err) {
+__device__ __forceinline__ uint32_t append_pos(uint32_t* counter, bool pred, uint32_t cap, uint32_t* err) {
     uint32_t b = __ballot_sync(0xffffffffu, pred);
-    if (!b) return;
+    if (!b) return kInvalidSlot;
     uint32_t lane = threadIdx.x & 31u;
     uint32_t leader = __ffs(b) - 1;
     uint32_t base = 0;
     if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(b));
     base = __shfl_sync(0xffffffffu, base, leader);
     uint32_t pos = base + __popc(b & ((1u << lane) - 1u));
-    if (pred) {
-        if (pos < cap) q[pos] = value;
-        else atomicOr(err, kErrQueueOverflow);
+    if (pred && pos >= cap) {
+        atomicOr(err, kErrQueueOverflow);
+        return kInvalidSlot;
     }
+    return pred ? pos : kInvalidSlot;
 }
 
 __global__ void k_control(Queues q) {
@@ -52,16 +55,15 @@ __global__ void k_control(Queues q) {
     for (int b = 0; b < kNumBuckets; ++b) c->bucket[b].v = 0;
     c->fetchExtension.v = 0;
     c->fetchShadow.v = 0;
-    unsigned long long remaining = c->totalWork - c->nextWork;
-    if (c->freeCount.v > q.capacity || c->ext[cur].v > q.capacity || c->shd[cur].v > q.capacity) {
+    // every live path holds one extension or shadow entry: the rest is room for new ones
+    uint32_t live = c->ext[cur].v + c->shd[cur].v;
+    if (c->ext[cur].v > q.capacity || c->shd[cur].v > q.capacity || live > q.capacity) {
         c->error |= kErrQueueOverflow;
-        c->freeCount.v = 0;
+        live = q.capacity;
     }
-    uint32_t g = (uint32_t)min((unsigned long long)c->freeCount.v, remaining);
-    g = min(g, q.capacity - min(c->ext[cur].v, q.capacity));
+    unsigned long long remaining = c->totalWork - c->nextWork;
+    uint32_t g = (uint32_t)min((unsigned long long)(q.capacity - live), remaining);
     c->genCount = g;
-    c->genFreeBase = c->freeCount.v - g;
-    c->freeCount.v -= g;
     c->genWorkBase = c->nextWork;
     c->nextWork += g;
     c->genExtBase = c->ext[cur].v;
@@ -75,14 +77,14 @@ __global__ void k_control(Queues q) {
 void launch_control(const Queues& q, cudaStream_t st) { k_control<<<1, 1, 0, st>>>(q); }
 
 // Camera ray for (pixel, sample): trace.cu:54-125.
-__global__ void __launch_bounds__(kShadeBlock) k_generate(Queues q, PathSoA p, Frame f) {
+__global__ void __launch_bounds__(kShadeBlock) k_generate(Queues q, Frame f) {
     Counters* c = q.ctr;
     const uint32_t g = c->genCount;
-    const uint32_t cur = c->cur;
-    const uint32_t fb = c->genFreeBase, eb = c->genExtBase;
+    const uint32_t eb = c->genExtBase;
+    const PathQ o = c->cur ? q.ext[1] : q.ext[0];
     const unsigned long long wb = c->genWorkBase;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g; i += gridDim.x * blockDim.x) {
-        uint32_t slot = q.freeStack[fb + i];
+        const uint32_t e = eb + i;
         unsigned long long w = wb + i;
         uint32_t sample = f.sampleOffset + (uint32_t)(w / f.perSample);
         uint32_t j = (uint32_t)(w % f.perSample);
@@ -105,29 +107,29 @@ __global__ void __launch_bounds__(kShadeBlock) k_generate(Queues q, PathSoA p, F
         float3 fwd = f3(f.fwd[0], f.fwd[1], f.fwd[2]), rt = f3(f.right[0], f.right[1], f.right[2]),
                up = f3(f.up[0], f.up[1], f.up[2]), pos = f3(f.pos[0], f.pos[1], f.pos[2]);
         float3 dir = normalize(add(add(fwd, mul(mul(rt, nx), f.tanHalf)), mul(mul(up, ny), f.tanHalf)));
-        float3 o = pos, d = dir;
+        float3 ro = pos, rd = dir;
         if (f.lens > 0.0f && f.focal > 0.0f) {
             float r3 = lcg_randf(js), r4 = lcg_randf(js);
             float th = 2.0f * 3.14159265f * r3;
             float rad = sqrtf(r4) * f.lens;
-            float ct = cosf(th), sn = sinf(th);
+            float sn, ct;
+            sincosf(th, &sn, &ct);
             float3 off = f3(rt.x * rad * ct + up.x * rad * sn, rt.y * rad * ct + up.y * rad * sn,
                             rt.z * rad * ct + up.z * rad * sn);
             float3 fp = f3(pos.x + dir.x * f.focal, pos.y + dir.y * f.focal, pos.z + dir.z * f.focal);
-            o = f3(pos.x + off.x, pos.y + off.y, pos.z + off.z);
-            d = normalize(f3(fp.x - o.x, fp.y - o.y, fp.z - o.z));
+            ro = f3(pos.x + off.x, pos.y + off.y, pos.z + off.z);
+            rd = normalize(f3(fp.x - ro.x, fp.y - ro.y, fp.z - ro.z));
         }
-        p.ray_o[slot] = make_float4(o.x, o.y, o.z, 0.0001f);
-        p.ray_d[slot] = make_float4(d.x, d.y, d.z, 1e20f);
-        p.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-        p.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(pixel));
-        p.st[slot] = make_uint4(seed, 0u, 0u, kFlagFirstHit | kFlagPrevDelta);
-        q.ext[cur][eb + i] = slot;
+        o.ray_o[e] = make_float4(ro.x, ro.y, ro.z, 0.0001f);
+        o.ray_d[e] = make_float4(rd.x, rd.y, rd.z, 1e20f);
+        o.thr[e] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+        o.rad[e] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(pixel));
+        o.st[e] = make_uint4(seed, 0u, 0u, kFlagFirstHit | kFlagPrevDelta);
     }
 }
 
-void launch_generate(const Queues& q, const PathSoA& p, const Frame& f, int grid, cudaStream_t st) {
-    k_generate<<<grid, kShadeBlock, 0, st>>>(q, p, f);
+void launch_generate(const Queues& q, const Frame& f, int grid, cudaStream_t st) {
+    k_generate<<<grid, kShadeBlock, 0, st>>>(q, f);
 }
 
 // ---------------------------------------------------------------------------
@@ -206,7 +208,7 @@ __device__ __forceinline__ float3 normal_mapped(const DevScene& s, const wrk_mat
     return h.n;
 }
 
-enum : int { kOutNone = 0, kOutExt = 1, kOutShadow = 2, kOutFree = 3 };
+enum : int { kOutNone = 0, kOutExt = 1, kOutShadow = 2, kOutDone = 3 };
 
 struct PathRegs {
     float3 o, d, thr, rad;
@@ -226,7 +228,7 @@ __device__ __forceinline__ int next_bounce(const Frame& f, PathRegs& r, const Hi
     r.depth += 1;
     if (r.depth >= f.maxBounces) {
         accumulate(f, r);
-        return kOutFree;
+        return kOutDone;
     }
     return kOutExt;
 }
@@ -278,11 +280,22 @@ __device__ __forceinline__ bool sample_light(const DevScene& s, PathRegs& r, con
     return true;
 }
 
+// A Lambert hit that sends a shadow ray: the shadow ray and contribution, plus the
+// entry (ray and hit record) the path resumes from after the visibility test.
+struct ShadowOut {
+    float3 o, d, c;
+    float dist;
+    float4 o4, d4, h4;
+};
+
+// Shades entry i of a bucket; the path's next state is left in r (and so for a
+// shadow ray).  Returns kOutExt / kOutShadow for a continuing path, kOutDone when
+// it ended (accumulated or dropped).
 template <uint32_t kBucket>
-__device__ __forceinline__ int shade_one(const DevScene& s, const PathSoA& p, const Frame& f, uint32_t slot) {
-    float4 o4 = p.ray_o[slot], d4 = p.ray_d[slot], h4 = p.hit[slot], t4 = p.thr[slot], r4 = p.rad[slot];
-    uint4 st = p.st[slot];
-    PathRegs r;
+__device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uint32_t i, const Frame& f, PathRegs& r,
+                                         ShadowOut& so) {
+    float4 o4 = in.ray_o[i], d4 = in.ray_d[i], h4 = in.hit[i], t4 = in.thr[i], r4 = in.rad[i];
+    uint4 st = in.st[i];
     r.o = f3(o4.x, o4.y, o4.z);
     r.d = f3(d4.x, d4.y, d4.z);
     r.thr = f3(t4.x, t4.y, t4.z);
@@ -298,7 +311,7 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathSoA& p, co
     uint32_t prim = __float_as_uint(h4.y);
     if (prim >= s.numTris) {
         atomicOr(f.err, kErrBadIndex);
-        return kOutFree;
+        return kOutDone;
     }
     HitAttr h = hit_program(s, r.o, r.d, h4.x, prim, mat);
     const bool matOk = mat < s.numMats;
@@ -313,8 +326,8 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathSoA& p, co
     }
     int out = kOutNone;
     if (kBucket == kBucketOther) {
-        if (!matOk) return kOutFree;  // shade.cu:35-38: terminated without accumulation
-        const wrk_material m = s.mats[mat];
+        if (!matOk) return kOutDone;  // shade.cu:35-38: terminated without accumulation
+        const wrk_material& m = s.mats[mat];
         if (m.type == kEmissive) {  // emission with MIS (trace.cu:288-316)
             float w = 1.0f;
             if (f.useNEE && r.depth > 0 && !(r.flags & kFlagPrevDelta) && s.numEmissive > 0) {
@@ -329,9 +342,9 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathSoA& p, co
             r.rad = add(r.rad, mul(mul(r.thr, em), w));
         }
         accumulate(f, r);  // shadeEmissive / default branch: terminateRay
-        return kOutFree;
+        return kOutDone;
     }
-    const wrk_material m = s.mats[mat];
+    const wrk_material& m = s.mats[mat];
     if (m.normalTextureId > 0) h.n = normal_mapped(s, m, h);
     if (kBucket == kBucketLambert) {
         // getMaterialAlbedo is a pure function of (material, uv): fetch it once
@@ -345,10 +358,13 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathSoA& p, co
                 float3 con = f3(r.thr.x * fb.x * ls.le.x * w / ls.lpdf, r.thr.y * fb.y * ls.le.y * w / ls.lpdf,
                                 r.thr.z * fb.z * ls.le.z * w / ls.lpdf);
                 if (finite3(con) && con.x >= 0.0f && con.y >= 0.0f && con.z >= 0.0f) {
-                    float3 so = offset_origin(h.pos, h.n, ls.toLight);
-                    p.sh_o[slot] = make_float4(so.x, so.y, so.z, 1e-5f);
-                    p.sh_d[slot] = make_float4(ls.toLight.x, ls.toLight.y, ls.toLight.z, ls.dist - 1e-5f);
-                    p.sh_c[slot] = make_float4(con.x, con.y, con.z, 0.0f);
+                    so.o = offset_origin(h.pos, h.n, ls.toLight);
+                    so.d = ls.toLight;
+                    so.dist = ls.dist;
+                    so.c = con;
+                    so.o4 = o4;
+                    so.d4 = d4;
+                    so.h4 = h4;
                     r.flags |= kFlagNeeDone;
                     out = kOutShadow;
                 }
@@ -366,7 +382,7 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathSoA& p, co
             r.thr = mul(r.thr, al);
             r.prevPdf = pdf;
             r.flags &= ~kFlagPrevDelta;
-            if (!rr(f, r, false)) return kOutFree;
+            if (!rr(f, r, false)) return kOutDone;
             out = next_bounce(f, r, h, wd);
         }
     } else if (kBucket == kBucketDielectric) {
@@ -397,7 +413,7 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathSoA& p, co
             }
         }
         r.flags |= kFlagPrevDelta;
-        if (!rr(f, r, true)) return kOutFree;
+        if (!rr(f, r, true)) return kOutDone;
         out = next_bounce(f, r, h, r.d);
     } else {  // GGX reflection
         float3 wo = neg(r.d);
@@ -425,72 +441,75 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathSoA& p, co
         float ct = dot(h.n, wi);
         if (pdf < 1e-5f || ct <= 0.0f) {
             accumulate(f, r);
-            return kOutFree;
+            return kOutDone;
         }
         float3 fb = ggx_eval(wo, wi, h.n, alb, m.roughness, m.metallic, m.ior);
         if (!finite3(fb)) {
             accumulate(f, r);
-            return kOutFree;
+            return kOutDone;
         }
         r.thr = f3(r.thr.x * fb.x * ct / pdf, r.thr.y * fb.y * ct / pdf, r.thr.z * fb.z * ct / pdf);
         r.prevPdf = pdf;
         r.flags &= ~kFlagPrevDelta;
-        if (!rr(f, r, false)) return kOutFree;
+        if (!rr(f, r, false)) return kOutDone;
         out = next_bounce(f, r, h, wi);
     }
-    // continuing path: iteration cap (renderer.cpp:213) then write back
+    // continuing path: the reference's host loop stops after maxIter iterations
+    // (renderer.cpp:213) and drops whatever is still alive
     if (out == kOutExt || out == kOutShadow) {
-        if (r.iter + 1u >= f.maxIter) return kOutFree;  // dropped, nothing accumulated
+        if (r.iter + 1u >= f.maxIter) return kOutDone;  // dropped, nothing accumulated
         r.iter += 1u;
-        if (out == kOutExt) {
-            p.ray_o[slot] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
-            p.ray_d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 1e20f);
-        }
-        p.thr[slot] = make_float4(r.thr.x, r.thr.y, r.thr.z, r.prevPdf);
-        p.rad[slot] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
-        p.st[slot] = make_uint4(r.seed, r.dim, (r.depth & 0xffffu) | (r.iter << 16), r.flags);
     }
     return out;
 }
 
+#ifndef WRK_SHADE_MIN_BLOCKS
+#define WRK_SHADE_MIN_BLOCKS 4
+#endif
 template <uint32_t kBucket>
-__global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, Queues q, PathSoA p, Frame f) {
+__global__ void __launch_bounds__(kShadeBlock, WRK_SHADE_MIN_BLOCKS) k_shade(DevScene s, Queues q, Frame f) {
     Counters* c = q.ctr;
     const uint32_t cur = c->cur, nxt = cur ^ 1u;
     const uint32_t n = min(c->bucket[kBucket].v, q.capacity);
-    const uint32_t* in = q.bucket[kBucket];
+    const PathQ in = q.bucket[kBucket];
+    const PathQ ext = nxt ? q.ext[1] : q.ext[0];
+    const PathQ shd = nxt ? q.shd[1] : q.shd[0];
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        uint32_t i = base + threadIdx.x;
-        uint32_t slot = i < n ? in[i] : kInvalidSlot;
-        if (slot != kInvalidSlot && slot >= q.capacity) {
-            atomicOr(&c->error, kErrBadIndex);
-            slot = kInvalidSlot;
-        }
+        const uint32_t i = base + threadIdx.x;
         constexpr uint32_t kCode = kBucket == kBucketLambertResume ? kBucketLambert : kBucket;
-        int out = slot != kInvalidSlot ? shade_one<kCode>(s, p, f, slot) : kOutNone;
-        warp_append_r(q.ext[nxt], &c->ext[nxt].v, out == kOutExt, slot, q.capacity, &c->error);
-        warp_append_r(q.shd[nxt], &c->shd[nxt].v, out == kOutShadow, slot, q.capacity, &c->error);
-        warp_append_r(q.freeStack, &c->freeCount.v, out == kOutFree, slot, q.capacity, &c->error);
+        PathRegs r;
+        ShadowOut so;
+        int out = i < n ? shade_one<kCode>(s, in, i, f, r, so) : kOutNone;
+        uint32_t pe = append_pos(&c->ext[nxt].v, out == kOutExt, q.capacity, &c->error);
+        uint32_t ps = append_pos(&c->shd[nxt].v, out == kOutShadow, q.capacity, &c->error);
+        if (pe != kInvalidSlot) {
+            ext.ray_o[pe] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
+            ext.ray_d[pe] = make_float4(r.d.x, r.d.y, r.d.z, 1e20f);
+            ext.thr[pe] = make_float4(r.thr.x, r.thr.y, r.thr.z, r.prevPdf);
+            ext.rad[pe] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
+            ext.st[pe] = make_uint4(r.seed, r.dim, (r.depth & 0xffffu) | (r.iter << 16), r.flags);
+        } else if (ps != kInvalidSlot) {
+            shd.ray_o[ps] = so.o4;
+            shd.ray_d[ps] = so.d4;
+            shd.hit[ps] = so.h4;
+            shd.thr[ps] = make_float4(r.thr.x, r.thr.y, r.thr.z, r.prevPdf);
+            shd.rad[ps] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
+            shd.st[ps] = make_uint4(r.seed, r.dim, (r.depth & 0xffffu) | (r.iter << 16), r.flags);
+            shd.sh_o[ps] = make_float4(so.o.x, so.o.y, so.o.z, 1e-5f);
+            shd.sh_d[ps] = make_float4(so.d.x, so.d.y, so.d.z, so.dist - 1e-5f);
+            shd.sh_c[ps] = make_float4(so.c.x, so.c.y, so.c.z, 0.0f);
+        }
     }
 }
 
-void launch_shade_bucket(uint32_t b, const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid,
-                         cudaStream_t st) {
+void launch_shade_bucket(uint32_t b, const DevScene& s, const Queues& q, const Frame& f, int grid, cudaStream_t st) {
     switch (b) {
-        case kBucketLambert: k_shade<kBucketLambert><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
-        case kBucketDielectric: k_shade<kBucketDielectric><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
-        case kBucketGGX: k_shade<kBucketGGX><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
-        case kBucketLambertResume: k_shade<kBucketLambertResume><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
-        default: k_shade<kBucketOther><<<grid, kShadeBlock, 0, st>>>(s, q, p, f); break;
+        case kBucketLambert: k_shade<kBucketLambert><<<grid, kShadeBlock, 0, st>>>(s, q, f); break;
+        case kBucketDielectric: k_shade<kBucketDielectric><<<grid, kShadeBlock, 0, st>>>(s, q, f); break;
+        case kBucketGGX: k_shade<kBucketGGX><<<grid, kShadeBlock, 0, st>>>(s, q, f); break;
+        case kBucketLambertResume: k_shade<kBucketLambertResume><<<grid, kShadeBlock, 0, st>>>(s, q, f); break;
+        default: k_shade<kBucketOther><<<grid, kShadeBlock, 0, st>>>(s, q, f); break;
     }
-}
-
-void launch_shade(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid, cudaStream_t st) {
-    k_shade<kBucketLambert><<<grid, kShadeBlock, 0, st>>>(s, q, p, f);
-    k_shade<kBucketDielectric><<<grid, kShadeBlock, 0, st>>>(s, q, p, f);
-    k_shade<kBucketGGX><<<grid, kShadeBlock, 0, st>>>(s, q, p, f);
-    k_shade<kBucketOther><<<grid, kShadeBlock, 0, st>>>(s, q, p, f);
-    k_shade<kBucketLambertResume><<<grid, kShadeBlock, 0, st>>>(s, q, p, f);
 }
 
 // rgb = sum * (1/spp) as renderer.cpp:308-313; guides averaged unless raw.

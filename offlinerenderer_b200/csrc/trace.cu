@@ -49,6 +49,12 @@ __device__ __forceinline__ bool mt_rn(const Ray& r, float4 a, float4 b, float4 c
 
 __device__ __forceinline__ uint32_t byte_of(uint32_t w, int k) { return (w >> (8 * k)) & 0xffu; }
 
+// Byte k of w as a float without an int->float conversion: one byte permute
+// builds the bits 0x4B0000bb = 2^23 + b exactly, and 2^23 is subtracted.
+__device__ __forceinline__ float qbyte(uint32_t w, uint32_t k) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + k)) - 8388608.0f;
+}
+
 // Intersects the 8 children of a node; returns internal hits (permuted by octant)
 // and the triangle mask relative to triBase.
 __device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, uint32_t idx, const Ray& r,
@@ -77,16 +83,16 @@ __device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, 
     const float tfar_lim = tfar_max * 1.00000024f;
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
-        int k = s & 3;
+        const uint32_t k = s & 3;
         uint32_t xn = s < 4 ? xn0 : xn1, xf = s < 4 ? xf0 : xf1;
         uint32_t yn = s < 4 ? yn0 : yn1, yf = s < 4 ? yf0 : yf1;
         uint32_t zn = s < 4 ? zn0 : zn1, zf = s < 4 ? zf0 : zf1;
-        float t0x = fmaf((float)byte_of(xn, k), sx, ax);
-        float t1x = fmaf((float)byte_of(xf, k), sx, ax);
-        float t0y = fmaf((float)byte_of(yn, k), sy, ay);
-        float t1y = fmaf((float)byte_of(yf, k), sy, ay);
-        float t0z = fmaf((float)byte_of(zn, k), sz, az);
-        float t1z = fmaf((float)byte_of(zf, k), sz, az);
+        float t0x = fmaf(qbyte(xn, k), sx, ax);
+        float t1x = fmaf(qbyte(xf, k), sx, ax);
+        float t0y = fmaf(qbyte(yn, k), sy, ay);
+        float t1y = fmaf(qbyte(yf, k), sy, ay);
+        float t0z = fmaf(qbyte(zn, k), sz, az);
+        float t1z = fmaf(qbyte(zf, k), sz, az);
         float tn = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, r.tmin));
         float tf = fminf(fminf(t1x, t1y), fminf(t1z, tfar_lim));
         if (tn <= tf * 1.00000024f) {
@@ -258,22 +264,25 @@ void launch_occluded_query(const DevScene& s, const float* rays, uint32_t n, uin
 }
 
 // ---------------------------------------------------------------------------
-// Wavefront trace kernels.  Queue appends are warp-aggregated: one ballot per
-// destination queue, one atomicAdd by the lowest active lane, positions by popc.
-__device__ __forceinline__ void warp_append(uint32_t* q, uint32_t* counter, bool pred, uint32_t value,
-                                            uint32_t cap, uint32_t* err) {
+// Wavefront trace kernels.  A path's state travels with it: a lane reads its ray
+// from the input queue entry it fetched and, when the ray is done, copies the
+// whole entry into the next queue at the position a warp-aggregated append (one
+// ballot per destination, one atomicAdd by the lowest lane) handed out, so the
+// lanes of a warp write consecutive entries.
+__device__ __forceinline__ uint32_t warp_append_pos(uint32_t* counter, bool pred, uint32_t cap, uint32_t* err) {
     uint32_t b = __ballot_sync(0xffffffffu, pred);
-    if (!b) return;
+    if (!b) return kInvalidSlot;
     uint32_t lane = threadIdx.x & 31u;
     uint32_t leader = __ffs(b) - 1;
     uint32_t base = 0;
     if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(b));
     base = __shfl_sync(0xffffffffu, base, leader);
     uint32_t pos = base + __popc(b & ((1u << lane) - 1u));
-    if (pred) {
-        if (pos < cap) q[pos] = value;
-        else atomicOr(err, kErrQueueOverflow);
+    if (pred && pos >= cap) {
+        atomicOr(err, kErrQueueOverflow);
+        return kInvalidSlot;
     }
+    return pred ? pos : kInvalidSlot;
 }
 
 __device__ __forceinline__ uint32_t bucket_of(uint32_t type) {
@@ -286,12 +295,20 @@ __device__ __forceinline__ uint32_t bucket_of(uint32_t type) {
     }
 }
 
+__device__ __forceinline__ PathQ pick_bucket(const Queues& q, uint32_t b) {
+    switch (b) {
+        case kBucketLambert: return q.bucket[kBucketLambert];
+        case kBucketDielectric: return q.bucket[kBucketDielectric];
+        case kBucketGGX: return q.bucket[kBucketGGX];
+        default: return q.bucket[kBucketOther];
+    }
+}
+
 // Persistent traversal: each warp keeps its lanes busy by fetching new rays from
 // the queue (one warp-aggregated atomic on a per-launch fetch counter) whenever
 // fewer than kRefillAt lanes still have a ray in flight, instead of waiting for
 // the slowest ray of a fixed batch (Aila & Laine 2009, "Understanding the
-// efficiency of ray traversal on GPUs").  Finished lanes hand their results on
-// with warp-aggregated queue appends.
+// efficiency of ray traversal on GPUs").
 #ifndef WRK_REFILL_AT
 #define WRK_REFILL_AT 16
 #endif
@@ -302,17 +319,17 @@ constexpr int kRefillAt = WRK_REFILL_AT;
 
 template <bool kAnyHit>
 __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_persistent(DevScene s, Queues q,
-                                                                                      PathSoA p, Frame f) {
+                                                                                      Frame f) {
     __shared__ uint2 sstack[kStackSmem * kTraceBlock];
     uint2 lstack[kStackLocal];
     Counters* c = q.ctr;
     const uint32_t cur = c->cur;
     const uint32_t n = min(kAnyHit ? c->shd[cur].v : c->ext[cur].v, q.capacity);
-    const uint32_t* in = kAnyHit ? q.shd[cur] : q.ext[cur];
+    const PathQ in = kAnyHit ? q.shd[cur] : q.ext[cur];
     uint32_t* fetch = kAnyHit ? &c->fetchShadow.v : &c->fetchExtension.v;
     const uint32_t lane = threadIdx.x & 31u;
     Trav t;
-    uint32_t slot = kInvalidSlot;
+    uint32_t idx = 0;
     bool active = false, exhausted = false;
     while (true) {
         uint32_t idle = __ballot_sync(0xffffffffu, !active && !exhausted);
@@ -321,17 +338,12 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
             if (lane == leader) base = atomicAdd(fetch, (uint32_t)__popc(idle));
             base = __shfl_sync(0xffffffffu, base, leader);
             if (!active && !exhausted) {
-                uint32_t idx = base + __popc(idle & ((1u << lane) - 1u));
+                idx = base + __popc(idle & ((1u << lane) - 1u));
                 if (idx < n) {
-                    slot = in[idx];
-                    if (slot < q.capacity) {
-                        float4 o = kAnyHit ? p.sh_o[slot] : p.ray_o[slot];
-                        float4 d = kAnyHit ? p.sh_d[slot] : p.ray_d[slot];
-                        trav_init(t, Ray{o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w});
-                        active = true;
-                    } else {
-                        atomicOr(&c->error, kErrBadIndex);
-                    }
+                    float4 o = kAnyHit ? in.sh_o[idx] : in.ray_o[idx];
+                    float4 d = kAnyHit ? in.sh_d[idx] : in.ray_d[idx];
+                    trav_init(t, Ray{o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w});
+                    active = true;
                 } else {
                     exhausted = true;
                 }
@@ -348,44 +360,61 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
         if (kAnyHit) {
             // Shadow stage of __raygen__trace (trace.cu:27-51): add the NEE
             // contribution if nothing lies in [tmin, tmax], then resume shading.
-            if (done && t.pBest == kNoHit) {
-                float4 rd = p.rad[slot], cc = p.sh_c[slot];
-                p.rad[slot] = make_float4(rd.x + cc.x, rd.y + cc.y, rd.z + cc.z, rd.w);
+            const PathQ& o = q.bucket[kBucketLambertResume];
+            uint32_t pos = warp_append_pos(&c->bucket[kBucketLambertResume].v, done, q.capacity, &c->error);
+            if (done && pos != kInvalidSlot) {
+                float4 rd = in.rad[idx];
+                if (t.pBest == kNoHit) {
+                    float4 cc = in.sh_c[idx];
+                    rd = make_float4(rd.x + cc.x, rd.y + cc.y, rd.z + cc.z, rd.w);
+                }
+                o.ray_o[pos] = in.ray_o[idx];
+                o.ray_d[pos] = in.ray_d[idx];
+                o.hit[pos] = in.hit[idx];
+                o.thr[pos] = in.thr[idx];
+                o.rad[pos] = rd;
+                o.st[pos] = in.st[idx];
             }
-            warp_append(q.bucket[kBucketLambertResume], &c->bucket[kBucketLambertResume].v, done, slot, q.capacity,
-                        &c->error);
         } else {
             uint32_t bucket = kNumBuckets;
-            bool miss = false;
+            float4 th = make_float4(0, 0, 0, 0), rd = make_float4(0, 0, 0, 0);
             if (done) {
+                th = in.thr[idx];
+                rd = in.rad[idx];
                 if (t.pBest != kNoHit) {
-                    p.hit[slot] = make_float4(t.tBest, __uint_as_float(t.pBest), __uint_as_float(t.mBest), 0.0f);
                     bucket = t.mBest < s.numMats ? bucket_of(s.mats[t.mBest].type) : kBucketOther;
                 } else {
-                    // __miss__trace + the raygen miss branch (trace.cu:143-148)
-                    miss = true;
-                    float4 th = p.thr[slot], rd = p.rad[slot];
+                    // __miss__trace + the raygen miss branch (trace.cu:143-148): T*env, accumulate, terminate
                     float3 L = make_float3(rd.x + th.x * s.env[0], rd.y + th.y * s.env[1], rd.z + th.z * s.env[2]);
                     L = clamp_fireflies(L, f.fireflyClamp);
                     atomicAdd(f.accum + __float_as_uint(rd.w), make_float4(L.x, L.y, L.z, 0.0f));
                 }
             }
+            uint32_t pos = kInvalidSlot;
 #pragma unroll
-            for (uint32_t b = 0; b < kBucketLambertResume; ++b)
-                warp_append(q.bucket[b], &c->bucket[b].v, bucket == b, slot, q.capacity, &c->error);
-            warp_append(q.freeStack, &c->freeCount.v, miss, slot, q.capacity, &c->error);
+            for (uint32_t b = 0; b < kBucketLambertResume; ++b) {
+                uint32_t pb = warp_append_pos(&c->bucket[b].v, bucket == b, q.capacity, &c->error);
+                if (bucket == b) pos = pb;
+            }
+            if (pos != kInvalidSlot) {
+                const PathQ o = pick_bucket(q, bucket);
+                o.ray_o[pos] = make_float4(t.r.ox, t.r.oy, t.r.oz, t.r.tmin);
+                o.ray_d[pos] = make_float4(t.r.dx, t.r.dy, t.r.dz, t.r.tmax);
+                o.hit[pos] = make_float4(t.tBest, __uint_as_float(t.pBest), __uint_as_float(t.mBest), 0.0f);
+                o.thr[pos] = th;
+                o.rad[pos] = rd;
+                o.st[pos] = in.st[idx];
+            }
         }
         if (done) active = false;
     }
 }
 
-void launch_trace_extension(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid,
-                            cudaStream_t st) {
-    k_trace_persistent<false><<<grid, kTraceBlock, 0, st>>>(s, q, p, f);
+void launch_trace_extension(const DevScene& s, const Queues& q, const Frame& f, int grid, cudaStream_t st) {
+    k_trace_persistent<false><<<grid, kTraceBlock, 0, st>>>(s, q, f);
 }
-void launch_trace_shadow(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid,
-                         cudaStream_t st) {
-    k_trace_persistent<true><<<grid, kTraceBlock, 0, st>>>(s, q, p, f);
+void launch_trace_shadow(const DevScene& s, const Queues& q, const Frame& f, int grid, cudaStream_t st) {
+    k_trace_persistent<true><<<grid, kTraceBlock, 0, st>>>(s, q, f);
 }
 
 }  // namespace wrk

@@ -6,13 +6,19 @@
 //                      RGBA8 texels, emissive list + power CDF, the 8-wide BVH
 //                      (80 B nodes = 5 x uint4) and leaf-ordered triangle records
 //                      (48 B = 3 x float4: v0|prim, e1|material, e2).
-//   Path slots (SoA, one float4 / uint4 per field, 16-byte aligned so every access
-//   is one 16-byte vector load or store):
+//   Path queues: a path's state travels with it from queue to queue.  Every queue
+//   stores its entries SoA -- one array per field, one float4 / uint4 per entry --
+//   so a kernel reading entries i..i+31 of a field, or writing the consecutive
+//   positions a warp-aggregated append hands out, issues one coalesced 512-byte
+//   access per field.  Fields:
 //      ray_o (origin, tmin)   ray_d (direction, tmax)   hit (t, prim, material, -)
-//      thr (throughput, prevPdf)   rad (radiance, pixel)   st (seed, rngDim, depth|iter<<16, flags|sample<<8)
+//      thr (throughput, prevPdf)   rad (radiance, pixel)   st (seed, rngDim, depth|iter<<16, flags)
 //      sh_o / sh_d (shadow ray)    sh_c (NEE contribution)
-//   Queues: u32 slot lists -- extension and shadow queues (double-buffered across
-//   iterations), four material buckets, and the free-slot stack.
+//   Queues: extension (ray_o ray_d thr rad st) and shadow (all nine fields), each
+//   double-buffered across iterations, and five material buckets (ray_o ray_d hit
+//   thr rad st).  No slot indirection and no free list: a path occupies exactly one
+//   entry between iterations, so the room for new camera paths is the capacity
+//   minus the extension and shadow entries the last iteration produced.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -68,7 +74,8 @@ struct DevScene {
     uint32_t numNodes;
 };
 
-struct PathSoA {
+// One queue's entries, SoA.  Fields a queue does not carry are null.
+struct PathQ {
     float4* ray_o;
     float4* ray_d;
     float4* hit;
@@ -95,13 +102,12 @@ struct Counters {
     HotCounter ext[2];
     HotCounter shd[2];
     HotCounter bucket[kNumBuckets];
-    HotCounter freeCount;
     HotCounter fetchExtension;  // rays taken by the persistent traversal kernels this iteration
     HotCounter fetchShadow;
     uint32_t cur;          // which ext/shd buffer the current iteration consumes
     uint32_t genCount;     // paths generated this iteration
-    uint32_t genFreeBase;  // free-stack index of the first slot popped this iteration
     uint32_t genExtBase;   // extension-queue index where the generated paths go
+    uint32_t pad0;
     uint32_t iteration;
     uint32_t error;
     uint32_t pad[2];
@@ -115,10 +121,9 @@ struct Counters {
 };
 
 struct Queues {
-    uint32_t* ext[2];
-    uint32_t* shd[2];
-    uint32_t* bucket[kNumBuckets];
-    uint32_t* freeStack;
+    PathQ ext[2];
+    PathQ shd[2];
+    PathQ bucket[kNumBuckets];
     Counters* ctr;
     uint32_t capacity;
 };
@@ -127,7 +132,7 @@ struct Frame {
     float pos[3], fwd[3], right[3], up[3];
     float tanHalf, aspect, focal, lens;
     uint32_t width, height;
-    uint32_t tilesX, perSample;  // 8x4 pixel tiles; work items per sample (padded to whole tiles)
+    uint32_t tilesX, perSample;  // 8x4 pixel tiles across the image (0 = row order); work items per sample
     uint32_t spp, useNEE, maxBounces, seed, maxIter, sampleOffset;
     float rrStart, fireflyClamp;
     float4* accum;   // radiance sum per pixel
@@ -138,14 +143,11 @@ struct Frame {
 
 // ---- host-callable launchers (defined in the .cu files) ----
 void launch_control(const Queues& q, cudaStream_t st);
-void launch_generate(const Queues& q, const PathSoA& p, const Frame& f, int grid, cudaStream_t st);
-void launch_trace_extension(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid,
-                            cudaStream_t st);
-void launch_trace_shadow(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid,
+void launch_generate(const Queues& q, const Frame& f, int grid, cudaStream_t st);
+void launch_trace_extension(const DevScene& s, const Queues& q, const Frame& f, int grid, cudaStream_t st);
+void launch_trace_shadow(const DevScene& s, const Queues& q, const Frame& f, int grid, cudaStream_t st);
+void launch_shade_bucket(uint32_t bucket, const DevScene& s, const Queues& q, const Frame& f, int grid,
                          cudaStream_t st);
-void launch_shade(const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f, int grid, cudaStream_t st);
-void launch_shade_bucket(uint32_t bucket, const DevScene& s, const Queues& q, const PathSoA& p, const Frame& f,
-                         int grid, cudaStream_t st);
 void launch_resolve(const Frame& f, uint32_t rawGuides, float* rgb, float* albedo, float* normal, cudaStream_t st);
 
 // BVH build (bvh_build.cu)

@@ -67,7 +67,9 @@ __device__ __forceinline__ float3 cosine_hemisphere(float u1, float u2, float& p
     float th = 2.0f * kPi * u2;
     float z = sqrtf(fmaxf(0.0f, 1.0f - u1));
     pdf = z / kPi;
-    return f3(r * cosf(th), r * sinf(th), z);
+    float sn, cs;
+    sincosf(th, &sn, &cs);
+    return f3(r * cs, r * sn, z);
 }
 __device__ __forceinline__ float cosine_pdf(float c) { return fmaxf(0.0f, c / kPi); }
 __device__ __forceinline__ float3 sample_triangle(float u1, float u2, float3 a, float3 b, float3 c, float3& nrm,
@@ -190,7 +192,8 @@ __device__ __forceinline__ void ggx_sample(float3 wo, float3 n, float3 tg, float
     float r = sqrtf(u0);
     bool lower = u1 < ia;
     float phi = kPi * (lower ? u1 / ia : 1.0f + (u1 - ia) / (1.0f - ia));
-    float sp = sinf(phi), cp = cosf(phi);
+    float sp, cp;
+    sincosf(phi, &sp, &cp);
     float p1 = r * cp;
     float p2 = r * sp * (lower ? 1.0f : sv.z);
     float sq = sqrtf(fmaxf(0.0f, 1.0f - (p1 * p1 + p2 * p2)));
