@@ -141,6 +141,11 @@ int wrk_scene_bvh_info(wrk_scene* s, wrk_bvh_info* info);
 /* Light list / CDF readback (getEmissiveTrianglesBuffer, getEmissiveTriangleCDFBuffer). */
 int wrk_scene_light_cdf(wrk_scene* s, uint32_t* tris, float* cdf, uint32_t capacity, uint32_t* count);
 
+/* Copies the 8-wide BVH to host memory for inspection: nodes = numNodes * 20 u32
+ * (five 16-byte words each), tris = numTriangles * 12 floats (v0|prim, e1|material,
+ * e2|0 per triangle, in leaf order).  Sizes come from wrk_scene_bvh_info. */
+int wrk_scene_bvh_export(wrk_scene* s, uint32_t* nodes, float* tris);
+
 /* Device addresses of a finalized scene's buffers: the getters of wr::Scene
  * (libWR/include/wr/scene.h:70-93); bvhNodes stands in for the GAS handle. */
 typedef struct {

@@ -380,6 +380,14 @@ int wrk_scene_light_cdf(wrk_scene* s, uint32_t* tris, float* cdf, uint32_t capac
     return WRK_OK;
 }
 
+int wrk_scene_bvh_export(wrk_scene* s, uint32_t* nodes, float* tris) {
+    int rc = check_scene(s);
+    if (rc) return rc;
+    if (nodes) CK(cudaMemcpy(nodes, s->nodes, sizeof(uint4) * 5 * (size_t)s->info.numNodes, cudaMemcpyDeviceToHost));
+    if (tris) CK(cudaMemcpy(tris, s->tris, sizeof(float4) * 3 * (size_t)s->info.numTriangles, cudaMemcpyDeviceToHost));
+    return WRK_OK;
+}
+
 int wrk_scene_buffers_get(wrk_scene* s, wrk_scene_buffers* o) {
     int rc = check_scene(s);
     if (rc) return rc;

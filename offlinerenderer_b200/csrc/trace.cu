@@ -27,23 +27,24 @@ struct Ray {
     float ox, oy, oz, dx, dy, dz, tmin, tmax;
 };
 
+// Moller-Trumbore without the reciprocal: barycentric numerators are compared
+// with det (sign-aware) and t is divided only for hits inside the triangle.
 __device__ __forceinline__ bool mt_rn(const Ray& r, float4 a, float4 b, float4 c, float& t) {
-    // pvec = d x e2, det = e1 . pvec, tvec = o - v0, u = tvec.pvec / det ...
     float px = __fsub_rn(__fmul_rn(r.dy, c.z), __fmul_rn(r.dz, c.y));
     float py = __fsub_rn(__fmul_rn(r.dz, c.x), __fmul_rn(r.dx, c.z));
     float pz = __fsub_rn(__fmul_rn(r.dx, c.y), __fmul_rn(r.dy, c.x));
     float det = __fadd_rn(__fadd_rn(__fmul_rn(b.x, px), __fmul_rn(b.y, py)), __fmul_rn(b.z, pz));
-    if (det == 0.0f) return false;
-    float inv = __frcp_rn(det);
     float sx = __fsub_rn(r.ox, a.x), sy = __fsub_rn(r.oy, a.y), sz = __fsub_rn(r.oz, a.z);
-    float u = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(sx, px), __fmul_rn(sy, py)), __fmul_rn(sz, pz)), inv);
-    if (!(u >= 0.0f && u <= 1.0f)) return false;
+    float un = __fadd_rn(__fadd_rn(__fmul_rn(sx, px), __fmul_rn(sy, py)), __fmul_rn(sz, pz));
     float qx = __fsub_rn(__fmul_rn(sy, b.z), __fmul_rn(sz, b.y));
     float qy = __fsub_rn(__fmul_rn(sz, b.x), __fmul_rn(sx, b.z));
     float qz = __fsub_rn(__fmul_rn(sx, b.y), __fmul_rn(sy, b.x));
-    float v = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(r.dx, qx), __fmul_rn(r.dy, qy)), __fmul_rn(r.dz, qz)), inv);
-    if (!(v >= 0.0f && __fadd_rn(u, v) <= 1.0f)) return false;
-    t = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(c.x, qx), __fmul_rn(c.y, qy)), __fmul_rn(c.z, qz)), inv);
+    float vn = __fadd_rn(__fadd_rn(__fmul_rn(r.dx, qx), __fmul_rn(r.dy, qy)), __fmul_rn(r.dz, qz));
+    float uv = __fadd_rn(un, vn);
+    bool inside = det > 0.0f ? (un >= 0.0f && vn >= 0.0f && uv <= det)
+                             : (det < 0.0f && un <= 0.0f && vn <= 0.0f && uv >= det);
+    if (!inside) return false;
+    t = __fdiv_rn(__fadd_rn(__fadd_rn(__fmul_rn(c.x, qx), __fmul_rn(c.y, qy)), __fmul_rn(c.z, qz)), det);
     return true;
 }
 

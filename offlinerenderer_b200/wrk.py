@@ -84,6 +84,7 @@ SIGNATURES = {
     "wrk_scene_bvh_info": ([_VP, C.POINTER(BvhInfoC)], _I),
     "wrk_scene_light_cdf": ([_VP, _VP, _VP, _U32, C.POINTER(_U32)], _I),
     "wrk_scene_buffers_get": ([_VP, _VP], _I),
+    "wrk_scene_bvh_export": ([_VP, _VP, _VP], _I),
     "wrk_renderer_create": ([_I, _U32, C.POINTER(_VP)], _I),
     "wrk_renderer_destroy": ([_VP], _I),
     "wrk_render": ([_VP, _VP, C.POINTER(CameraC), C.POINTER(RenderParamsC), _VP, _VP, _VP,
@@ -287,6 +288,14 @@ class Scene:
         info = BvhInfoC()
         _check(lib().wrk_scene_bvh_info(self.handle, C.byref(info)))
         return {k: getattr(info, k) for k, _ in BvhInfoC._fields_}
+
+    def bvh_export(self):
+        """(nodes (N,20) u32, tris (T,12) f32) of the 8-wide BVH as built on the device."""
+        info = self.bvh_info()
+        nodes = np.zeros((info["numNodes"], 20), np.uint32)
+        tris = np.zeros((info["numTriangles"], 12), np.float32)
+        _check(lib().wrk_scene_bvh_export(self.handle, nodes.ctypes.data, tris.ctypes.data))
+        return nodes, tris
 
     def light_cdf(self):
         n = C.c_uint32()

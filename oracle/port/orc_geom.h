@@ -223,8 +223,11 @@ inline void build_bvh(Scene& s) {
     }
 }
 
-// Moller-Trumbore, FP32.  The CUDA trace kernel evaluates the same expression
-// sequence on the same per-triangle (v0, v1-v0, v2-v0) values, so t is bit-identical.
+// Moller-Trumbore, FP32, without the reciprocal: the barycentric tests compare the
+// numerators u*det and v*det against det (sign-aware), and t = t_num / det is
+// divided (correctly rounded) only for hits inside the triangle.  The CUDA trace
+// kernel evaluates the same expression sequence on the same per-triangle
+// (v0, v1-v0, v2-v0) values, so t is bit-identical.
 inline bool mt32(const float o[3], const float d[3], const float* v0, const float* e1, const float* e2,
                         float& t) {
     float px = d[1] * e2[2] - d[2] * e2[1];
@@ -232,16 +235,16 @@ inline bool mt32(const float o[3], const float d[3], const float* v0, const floa
     float pz = d[0] * e2[1] - d[1] * e2[0];
     float det = e1[0] * px + e1[1] * py + e1[2] * pz;
     if (det == 0.0f) return false;
-    float inv = 1.0f / det;
     float sx = o[0] - v0[0], sy = o[1] - v0[1], sz = o[2] - v0[2];
-    float u = (sx * px + sy * py + sz * pz) * inv;
-    if (!(u >= 0.0f && u <= 1.0f)) return false;
+    float un = sx * px + sy * py + sz * pz;
     float qx = sy * e1[2] - sz * e1[1];
     float qy = sz * e1[0] - sx * e1[2];
     float qz = sx * e1[1] - sy * e1[0];
-    float v = (d[0] * qx + d[1] * qy + d[2] * qz) * inv;
-    if (!(v >= 0.0f && u + v <= 1.0f)) return false;
-    t = (e2[0] * qx + e2[1] * qy + e2[2] * qz) * inv;
+    float vn = d[0] * qx + d[1] * qy + d[2] * qz;
+    float uv = un + vn;
+    bool inside = det > 0.0f ? (un >= 0.0f && vn >= 0.0f && uv <= det) : (un <= 0.0f && vn <= 0.0f && uv >= det);
+    if (!inside) return false;
+    t = (e2[0] * qx + e2[1] * qy + e2[2] * qz) / det;
     return true;
 }
 
@@ -264,7 +267,9 @@ inline bool mt64(const double o[3], const double d[3], const double v0[3], const
 // Slab test with the far distance widened by a few ulps so that rounding never
 // culls a box whose triangles the exact test would hit.
 inline bool box_hit(const BNode& b, const float o[3], const float inv[3], float tmin, float tmax) {
-    float t0 = tmin, t1 = tmax;
+    // the current best t is widened too: a box reaching an equal-t hit must be
+    // opened so ties resolve to the lowest triangle index wherever they lie
+    float t0 = tmin, t1 = tmax * 1.0000005f;
     for (int k = 0; k < 3; ++k) {
         float a = (b.lo[k] - o[k]) * inv[k], c = (b.hi[k] - o[k]) * inv[k];
         float n = std::min(a, c), f = std::max(a, c);

@@ -618,3 +618,163 @@ uint32_t orc_compact(const uint32_t* stage, const uint32_t* idx, uint32_t n, uin
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Independent CPU reader of the library's 8-wide BVH format (test infrastructure):
+// decodes the exported nodes / leaf triangles and traverses them to count node
+// visits and triangle tests per ray, and returns the closest hit for comparison.
+namespace {
+struct Node8 {
+    float p[3];
+    int e[3];
+    uint32_t imask, childBase, triBase;
+    uint8_t meta[8], qlo[3][8], qhi[3][8];
+};
+Node8 decode8(const uint32_t* w) {
+    Node8 n;
+    for (int k = 0; k < 3; ++k) std::memcpy(&n.p[k], &w[k], 4);
+    for (int k = 0; k < 3; ++k) n.e[k] = (int)((w[3] >> (8 * k)) & 0xff) - 127;
+    n.imask = w[3] >> 24;
+    n.childBase = w[4];
+    n.triBase = w[5];
+    for (int s = 0; s < 8; ++s) n.meta[s] = (uint8_t)(w[6 + s / 4] >> (8 * (s % 4)));
+    const uint32_t* q = w + 8;  // qlox(2) qloy(2) qloz(2) qhix(2) qhiy(2) qhiz(2)
+    for (int a = 0; a < 3; ++a)
+        for (int s = 0; s < 8; ++s) {
+            n.qlo[a][s] = (uint8_t)(q[2 * a + s / 4] >> (8 * (s % 4)));
+            n.qhi[a][s] = (uint8_t)(q[6 + 2 * a + s / 4] >> (8 * (s % 4)));
+        }
+    return n;
+}
+}  // namespace
+
+extern "C" {
+
+// Checks structural invariants; returns 0 if all hold, else a code (1 bad index,
+// 2 triangle outside its child box, 3 triangle referenced not exactly once).
+// out[0] = max depth, out[1] = internal child slots, out[2] = leaf child slots.
+int orc_bvh8_validate(const uint32_t* nodes, uint32_t nn, const float* tris, uint32_t nt, uint32_t* out) {
+    std::vector<uint32_t> seen(nt, 0);
+    std::vector<std::pair<uint32_t, uint32_t>> stack{{0, 1}};
+    uint32_t maxd = 0, ni = 0, nl = 0;
+    while (!stack.empty()) {
+        auto [idx, depth] = stack.back();
+        stack.pop_back();
+        if (idx >= nn) return 1;
+        maxd = std::max(maxd, depth);
+        Node8 n = decode8(nodes + 20 * (size_t)idx);
+        uint32_t rank = 0;
+        for (int s = 0; s < 8; ++s) {
+            bool empty = n.qlo[0][s] > n.qhi[0][s];
+            if (empty) continue;
+            double lo[3], hi[3];
+            for (int a = 0; a < 3; ++a) {
+                double sc = std::ldexp(1.0, n.e[a]);
+                lo[a] = n.p[a] + n.qlo[a][s] * sc;
+                hi[a] = n.p[a] + n.qhi[a][s] * sc;
+            }
+            if ((n.imask >> s) & 1u) {
+                stack.push_back({n.childBase + rank, depth + 1});
+                ++rank;
+                ++ni;
+            } else {
+                ++nl;
+                uint32_t cnt = (n.meta[s] >> 5) + 1, off = n.meta[s] & 31;
+                for (uint32_t k = 0; k < cnt; ++k) {
+                    uint32_t ti = n.triBase + off + k;
+                    if (ti >= nt) return 1;
+                    const float* t = tris + 12 * (size_t)ti;
+                    uint32_t prim;
+                    std::memcpy(&prim, &t[3], 4);
+                    if (prim >= nt) return 1;
+                    seen[prim]++;
+                    double v[3][3];
+                    for (int a = 0; a < 3; ++a) {
+                        v[0][a] = t[a];
+                        v[1][a] = (double)t[a] + t[4 + a];
+                        v[2][a] = (double)t[a] + t[8 + a];
+                    }
+                    for (int j = 0; j < 3; ++j)
+                        for (int a = 0; a < 3; ++a)
+                            if (v[j][a] < lo[a] - 1e-6 * (1 + std::fabs(lo[a])) ||
+                                v[j][a] > hi[a] + 1e-6 * (1 + std::fabs(hi[a])))
+                                return 2;
+                }
+            }
+        }
+    }
+    for (uint32_t c : seen)
+        if (c != 1) return 3;
+    out[0] = maxd;
+    out[1] = ni;
+    out[2] = nl;
+    return 0;
+}
+
+// Closest hit through the exported BVH (same traversal order as the GPU) with
+// per-ray node-visit and triangle-test counts.
+void orc_bvh8_trace(const uint32_t* nodes, uint32_t nn, const float* tris, uint32_t nt, const float* rays, uint32_t n,
+                    float* out_t, uint32_t* out_prim, uint32_t* visits, uint32_t* tests) {
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 256)
+#endif
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        const float* r = rays + 8 * i;
+        float o[3] = {r[0], r[1], r[2]}, d[3] = {r[4], r[5], r[6]};
+        float inv[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};
+        uint32_t octinv = ((d[0] < 0) | ((d[1] < 0) << 1) | ((d[2] < 0) << 2)) ^ 7u;
+        float tb = r[7];
+        uint32_t pb = 0xffffffffu, nv = 0, ntst = 0;
+        std::vector<uint32_t> stack{0};
+        while (!stack.empty()) {
+            uint32_t idx = stack.back();
+            stack.pop_back();
+            if (idx >= nn) break;
+            ++nv;
+            Node8 nd = decode8(nodes + 20 * (size_t)idx);
+            struct Hit { uint32_t key, slot; };
+            std::vector<Hit> hits;
+            uint32_t rank = 0;
+            uint32_t ranks[8];
+            for (int s = 0; s < 8; ++s) { ranks[s] = rank; if ((nd.imask >> s) & 1u) ++rank; }
+            for (int s = 0; s < 8; ++s) {
+                if (nd.qlo[0][s] > nd.qhi[0][s]) continue;
+                float t0 = r[3], t1 = tb * 1.0000005f;
+                for (int a = 0; a < 3; ++a) {
+                    double sc = std::ldexp(1.0, nd.e[a]);
+                    float lo = (float)(nd.p[a] + nd.qlo[a][s] * sc), hi = (float)(nd.p[a] + nd.qhi[a][s] * sc);
+                    float x = (lo - o[a]) * inv[a], y = (hi - o[a]) * inv[a];
+                    float mn = std::min(x, y), mx = std::max(x, y);
+                    if (mn != mn) mn = -INFINITY;
+                    if (mx != mx) mx = INFINITY;
+                    t0 = std::max(t0, mn);
+                    t1 = std::min(t1, mx * 1.0000005f);
+                }
+                if (t0 > t1) continue;
+                if ((nd.imask >> s) & 1u) {
+                    hits.push_back({(uint32_t)s ^ octinv, nd.childBase + ranks[s]});
+                } else {
+                    uint32_t cnt = (nd.meta[s] >> 5) + 1, off = nd.meta[s] & 31;
+                    for (uint32_t k = 0; k < cnt; ++k) {
+                        const float* t = tris + 12 * (size_t)(nd.triBase + off + k);
+                        float th;
+                        ++ntst;
+                        if (mt32(o, d, t, t + 4, t + 8, th) && th >= r[3] && th <= r[7]) {
+                            uint32_t prim;
+                            std::memcpy(&prim, &t[3], 4);
+                            if (th < tb || (th == tb && prim < pb)) { tb = th; pb = prim; }
+                        }
+                    }
+                }
+            }
+            std::sort(hits.begin(), hits.end(), [](const Hit& a, const Hit& b) { return a.key > b.key; });
+            for (auto& h : hits) stack.push_back(h.slot);  // lowest key popped first
+        }
+        out_t[i] = pb == 0xffffffffu ? INFINITY : tb;
+        out_prim[i] = pb;
+        visits[i] = nv;
+        tests[i] = ntst;
+    }
+}
+
+}  // extern "C"

@@ -227,6 +227,33 @@ class Oracle(_Base):
                                    C.c_void_p(out.ctypes.data))
         return out
 
+    def bvh8_validate(self, nodes: np.ndarray, tris: np.ndarray):
+        """Structural check of an exported 8-wide BVH; returns (code, depth, internal, leaf)."""
+        nodes = np.ascontiguousarray(nodes, np.uint32)
+        tris = np.ascontiguousarray(tris, np.float32)
+        out = np.zeros(3, np.uint32)
+        self.lib.orc_bvh8_validate.restype = C.c_int
+        rc = self.lib.orc_bvh8_validate(C.c_void_p(nodes.ctypes.data), C.c_uint32(nodes.shape[0]),
+                                        C.c_void_p(tris.ctypes.data), C.c_uint32(tris.shape[0]),
+                                        C.c_void_p(out.ctypes.data))
+        return int(rc), int(out[0]), int(out[1]), int(out[2])
+
+    def bvh8_trace(self, nodes: np.ndarray, tris: np.ndarray, rays: np.ndarray):
+        """Closest hit through an exported 8-wide BVH: (t, prim, node visits, triangle tests)."""
+        nodes = np.ascontiguousarray(nodes, np.uint32)
+        tris = np.ascontiguousarray(tris, np.float32)
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        t = np.zeros(n, np.float32)
+        p = np.zeros(n, np.uint32)
+        v = np.zeros(n, np.uint32)
+        k = np.zeros(n, np.uint32)
+        self.lib.orc_bvh8_trace(C.c_void_p(nodes.ctypes.data), C.c_uint32(nodes.shape[0]), C.c_void_p(tris.ctypes.data),
+                                C.c_uint32(tris.shape[0]), C.c_void_p(rays.ctypes.data), C.c_uint32(n),
+                                C.c_void_p(t.ctypes.data), C.c_void_p(p.ctypes.data), C.c_void_p(v.ctypes.data),
+                                C.c_void_p(k.ctypes.data))
+        return t, p, v, k
+
     def compact(self, stage, idx):
         stage = np.ascontiguousarray(stage, np.uint32)
         idx = np.ascontiguousarray(idx, np.uint32)

@@ -146,3 +146,16 @@ def test_errors_are_reported(gpu):
     bad = gpu.Scene()
     with pytest.raises(gpu.WrkError):
         bad.finalize()  # no geometry (scene.cpp:356-358)
+
+
+def test_sample_offset_split_equals_full_render(gpu):
+    """Renders of sample ranges [0, k) and [k, 2k) sum to the render of [0, 2k):
+    the sample split the multi-GPU bench uses."""
+    sd = scenes.material_showcase(40, 32, 8, seed=6, tex_size=64)
+    s = gpu.Scene.from_data(sd)
+    r = gpu.Renderer(capacity=1 << 15)
+    a = r.render(s, spp=4, sample_offset=0).rgb
+    b = r.render(s, spp=4, sample_offset=4).rgb
+    full = r.render(s, spp=8).rgb
+    np.testing.assert_allclose((a + b) * 0.5, full, rtol=1e-5, atol=1e-6)
+    assert np.abs(a - b).max() > 1e-3
