@@ -202,6 +202,46 @@ int wrk_camera_rays(const wrk_camera* cam, uint32_t width, uint32_t height, cons
 /* Exposure 2.2, ACES filmic fit, gamma 1/2.2, 8-bit (libWR/test/helpers/image.cpp:14-49). */
 int wrk_tonemap_aces(const float* d_rgb, uint32_t numPixels, uint8_t* d_out);
 
+/* ---- learned denoiser: replaces the OptiX AI denoiser of libWR
+ *      (libWR/src/internal/denoiser.cpp:17-195: optixDenoiserCreate :30-35,
+ *      guide layers :98-116, optixDenoiserInvoke :171-184) ---- */
+/* 3x3 convolution, stride 1, zero padding, on the tensor cores (bf16 in, f32
+ * accumulate).  x: bf16 NHWC [B][H][W][Cin]; w: bf16 [Cout][3][3][Cin]; bias: f32
+ * [Cout] or NULL; out: NHWC [B][H][W][Cout], bf16 or (flags & 2) f32; flags & 1 =
+ * ReLU.  Cin a multiple of 16, Cout <= 256, H a multiple of 8, W of 16; device
+ * pointers 16-byte aligned.  Kernel-level entry of the denoiser's convolution. */
+#define WRK_CONV_RELU 1u
+#define WRK_CONV_F32_OUT 2u
+int wrk_conv3x3_forward(const void* d_x, uint32_t B, uint32_t H, uint32_t W, uint32_t Cin, const void* d_w,
+                        const float* d_bias, uint32_t Cout, uint32_t flags, void* d_out);
+/* Weight gradient of that convolution: dw[Cout][3][3][Cin] (f32) += sum over pixels
+ * of g[p][co] * x[p + tap][ci]; g: bf16 NHWC [B][H][W][Cout]. */
+int wrk_conv3x3_wgrad(const void* d_g, const void* d_x, uint32_t B, uint32_t H, uint32_t W, uint32_t Cin,
+                      uint32_t Cout, float* d_dw);
+
+typedef struct wrk_denoiser wrk_denoiser;
+/* A 4-level U-Net (32/64/128/256 channels) on radiance + albedo + normal, weights
+ * initialised from `seed`.  Parameters are one f32 array: per layer W [Cout][3][3][Cin]
+ * then bias [Cout], layers in the order e0a e0b e1a e1b e2a e2b e3a e3b d2a d2b d1a
+ * d1b d0a d0b head. */
+int wrk_denoiser_create(int device, uint32_t seed, wrk_denoiser** out);
+int wrk_denoiser_destroy(wrk_denoiser* d);
+int wrk_denoiser_num_params(wrk_denoiser* d, uint64_t* n);
+int wrk_denoiser_get_params(wrk_denoiser* d, float* h_params, uint64_t n);
+/* Sets the weights (host array) and resets the optimizer state. */
+int wrk_denoiser_set_params(wrk_denoiser* d, const float* h_params, uint64_t n);
+/* One forward + backward pass on device images [B][H][W][3] f32 (rgb, albedo, normal,
+ * target; H a multiple of 64, W of 128): the L1 loss of log1p(radiance) and the
+ * parameter gradients (copied to h_grads when not NULL). */
+int wrk_denoiser_gradients(wrk_denoiser* d, const float* d_rgb, const float* d_albedo, const float* d_normal,
+                           const float* d_target, uint32_t B, uint32_t H, uint32_t W, float* h_grads, float* loss);
+/* The same followed by one Adam step with learning rate lr. */
+int wrk_denoiser_train_step(wrk_denoiser* d, const float* d_rgb, const float* d_albedo, const float* d_normal,
+                            const float* d_target, uint32_t B, uint32_t H, uint32_t W, float lr, float* loss);
+/* Denoises device images [B][H][W][3] f32 of any size (padded internally) into d_out. */
+int wrk_denoiser_infer(wrk_denoiser* d, const float* d_rgb, const float* d_albedo, const float* d_normal, uint32_t B,
+                       uint32_t H, uint32_t W, float* d_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -101,6 +101,16 @@ SIGNATURES = {
     "wrk_texture_batch": ([_VP, _U32, _VP, _U32, _VP], _I),
     "wrk_camera_rays": ([C.POINTER(CameraC), _U32, _U32, _VP, _VP, _U32, _U32, _VP], _I),
     "wrk_tonemap_aces": ([_VP, _U32, _VP], _I),
+    "wrk_conv3x3_forward": ([_VP, _U32, _U32, _U32, _U32, _VP, _VP, _U32, _U32, _VP], _I),
+    "wrk_conv3x3_wgrad": ([_VP, _VP, _U32, _U32, _U32, _U32, _U32, _VP], _I),
+    "wrk_denoiser_create": ([_I, _U32, C.POINTER(_VP)], _I),
+    "wrk_denoiser_destroy": ([_VP], _I),
+    "wrk_denoiser_num_params": ([_VP, C.POINTER(_U64)], _I),
+    "wrk_denoiser_get_params": ([_VP, _VP, _U64], _I),
+    "wrk_denoiser_set_params": ([_VP, _VP, _U64], _I),
+    "wrk_denoiser_gradients": ([_VP, _VP, _VP, _VP, _VP, _U32, _U32, _U32, _VP, C.POINTER(_F)], _I),
+    "wrk_denoiser_train_step": ([_VP, _VP, _VP, _VP, _VP, _U32, _U32, _U32, _F, C.POINTER(_F)], _I),
+    "wrk_denoiser_infer": ([_VP, _VP, _VP, _VP, _U32, _U32, _U32, _VP], _I),
 }
 
 _lib = None
@@ -442,3 +452,104 @@ def tonemap_aces(rgb: np.ndarray, device: int = 0) -> np.ndarray:
     do = DeviceArray(rgb.shape, np.uint8, device)
     _check(lib().wrk_tonemap_aces(di.ptr, npx, do.ptr))
     return do.numpy()
+
+
+# ---- learned denoiser ----
+def to_bf16_bits(a: np.ndarray) -> np.ndarray:
+    """f32 -> bf16 bit patterns (round to nearest even), as uint16."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32)
+    return ((u + (((u >> 16) & 1) + 0x7FFF)) >> 16).astype(np.uint16)
+
+
+def from_bf16_bits(b: np.ndarray) -> np.ndarray:
+    return (np.asarray(b, np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
+def conv3x3(x: np.ndarray, w: np.ndarray, bias=None, relu=False, f32_out=True, device: int = 0) -> np.ndarray:
+    """Tensor-core 3x3 convolution: x (B,H,W,Cin) and w (Cout,3,3,Cin) are rounded to
+    bf16; returns (B,H,W,Cout) f32 (or the bf16 result widened to f32)."""
+    B, H, W, Cin = x.shape
+    Cout = w.shape[0]
+    dx = DeviceArray.from_numpy(to_bf16_bits(x), device)
+    dw = DeviceArray.from_numpy(to_bf16_bits(w), device)
+    db = None if bias is None else DeviceArray.from_numpy(np.asarray(bias, np.float32), device)
+    do = DeviceArray((B, H, W, Cout), np.float32 if f32_out else np.uint16, device)
+    flags = (1 if relu else 0) | (2 if f32_out else 0)
+    _check(lib().wrk_conv3x3_forward(dx.ptr, B, H, W, Cin, dw.ptr, None if db is None else db.ptr, Cout, flags,
+                                     do.ptr))
+    out = do.numpy()
+    return out if f32_out else from_bf16_bits(out)
+
+
+def conv3x3_wgrad(g: np.ndarray, x: np.ndarray, device: int = 0) -> np.ndarray:
+    """dW (Cout,3,3,Cin) = sum_p g[p] x[p + tap] with g (B,H,W,Cout), x (B,H,W,Cin) in bf16."""
+    B, H, W, Cin = x.shape
+    Cout = g.shape[3]
+    dg = DeviceArray.from_numpy(to_bf16_bits(g), device)
+    dx = DeviceArray.from_numpy(to_bf16_bits(x), device)
+    dw = DeviceArray.from_numpy(np.zeros((Cout, 3, 3, Cin), np.float32), device)
+    _check(lib().wrk_conv3x3_wgrad(dg.ptr, dx.ptr, B, H, W, Cin, Cout, dw.ptr))
+    return dw.numpy()
+
+
+class Denoiser:
+    """The learned U-Net denoiser (stands in for libWR's OptiX AI denoiser)."""
+
+    def __init__(self, device: int = 0, seed: int = 1):
+        self.device = device
+        h = C.c_void_p()
+        _check(lib().wrk_denoiser_create(device, seed, C.byref(h)))
+        self.handle = h.value
+        n = C.c_uint64()
+        _check(lib().wrk_denoiser_num_params(self.handle, C.byref(n)))
+        self.num_params = n.value
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and _lib is not None:
+            _lib.wrk_denoiser_destroy(h)
+            self.handle = None
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.num_params, np.float32)
+        _check(lib().wrk_denoiser_get_params(self.handle, out.ctypes.data, self.num_params))
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        _check(lib().wrk_denoiser_set_params(self.handle, p.ctypes.data, p.size))
+
+    @staticmethod
+    def _ptr(a):
+        return None if a is None else a.ptr
+
+    def gradients(self, d_rgb, d_alb, d_nrm, d_target, B, H, W):
+        g = np.zeros(self.num_params, np.float32)
+        loss = C.c_float()
+        _check(lib().wrk_denoiser_gradients(self.handle, d_rgb.ptr, self._ptr(d_alb), self._ptr(d_nrm), d_target.ptr,
+                                            B, H, W, g.ctypes.data, C.byref(loss)))
+        return loss.value, g
+
+    def train_step(self, d_rgb, d_alb, d_nrm, d_target, B, H, W, lr: float) -> float:
+        loss = C.c_float()
+        _check(lib().wrk_denoiser_train_step(self.handle, d_rgb.ptr, self._ptr(d_alb), self._ptr(d_nrm), d_target.ptr,
+                                             B, H, W, lr, C.byref(loss)))
+        return loss.value
+
+    def infer_device(self, d_rgb, d_alb, d_nrm, B, H, W, d_out) -> None:
+        _check(lib().wrk_denoiser_infer(self.handle, d_rgb.ptr, self._ptr(d_alb), self._ptr(d_nrm), B, H, W,
+                                        d_out.ptr))
+
+    def infer(self, rgb: np.ndarray, albedo=None, normal=None) -> np.ndarray:
+        """Denoise host images (H,W,3) or (B,H,W,3)."""
+        rgb = np.asarray(rgb, np.float32)
+        squeeze = rgb.ndim == 3
+        r4 = rgb[None] if squeeze else rgb
+        B, H, W, _ = r4.shape
+        dr = DeviceArray.from_numpy(r4, self.device)
+        da = None if albedo is None else DeviceArray.from_numpy(np.asarray(albedo, np.float32).reshape(r4.shape), self.device)
+        dn = None if normal is None else DeviceArray.from_numpy(np.asarray(normal, np.float32).reshape(r4.shape), self.device)
+        do = DeviceArray(r4.shape, np.float32, self.device)
+        self.infer_device(dr, da, dn, B, H, W, do)
+        out = do.numpy()
+        return out[0] if squeeze else out
