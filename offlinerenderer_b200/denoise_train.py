@@ -1,0 +1,193 @@
+"""Training of the learned denoiser, on the GPU end to end.
+
+    python -m offlinerenderer_b200.denoise_train [--scenes 8] [--views 16] [--steps 3000] [--out PATH]
+
+The renderer itself generates the training pairs: seeded variants of the
+scale-test scene (heightfield + 250 icospheres of the five BSDFs + 64 emissive
+triangles; scene seeds 101.. -- the benchmark scene, seed 1, is held out),
+seen from the scale-test camera and from random orbit cameras (radius U(1,3)
+around the scene centre, the serving workload's poses).  For every view it
+renders a high-spp target and noisy inputs at 1..32 spp from disjoint sample
+indices (radiance + first-hit albedo + normal, the 9 channels libWR gives its
+denoiser, libWR/src/internal/denoiser.cpp:98-116).  Training takes random crops
+with random flips and runs the network's forward, backward and Adam step through
+wrk_denoiser_train_step (tcgen05 convolutions).  torch only holds the data in
+device memory and gathers the crops.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+from . import scenes, wrk
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_WEIGHTS = os.path.join(HERE, "weights", "unet_scale.npz")
+INPUT_SPPS = (1, 2, 4, 8, 16, 32)
+
+
+def relmse(x: np.ndarray, ref: np.ndarray) -> float:
+    """mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2)."""
+    x = np.asarray(x, np.float64)
+    r = np.asarray(ref, np.float64)
+    return float(np.mean((x - r) ** 2 / (r * r + 1e-2)))
+
+
+def orbit_camera(rng, width: int, height: int, center=(0.5, 0.05, 0.5)) -> scenes.Camera:
+    """Camera on an orbit of radius U(1,3) around the scene centre, looking at it."""
+    r = float(rng.uniform(1.0, 3.0))
+    th = float(rng.uniform(0.0, 2.0 * math.pi))
+    el = float(rng.uniform(math.radians(20.0), math.radians(55.0)))
+    c = np.asarray(center, np.float64)
+    pos = c + r * np.array([math.cos(el) * math.cos(th), math.sin(el), math.cos(el) * math.sin(th)])
+    fov = float(np.clip(2.0 * math.atan(0.8 / r), math.radians(15.0), math.radians(60.0)))
+    return scenes.Camera(position=tuple(float(v) for v in pos), target=tuple(float(v) for v in c), up=(0.0, 1.0, 0.0),
+                         fovY=fov, aspect=float(np.float32(width) / np.float32(height)))
+
+
+class _Ptr:
+    """Device address wrapper accepted wherever the binding takes a DeviceArray."""
+
+    def __init__(self, t):
+        self.t = t
+        self.ptr = t.data_ptr()
+
+
+def render_views(scene, renderer, cams, size, spp, sample_offset, torch, device):
+    """Renders every camera at `spp` into (V, size, size, 3) rgb / albedo / normal tensors."""
+    V = len(cams)
+    rgb = torch.empty((V, size, size, 3), dtype=torch.float32, device=f"cuda:{device}")
+    alb = torch.empty_like(rgb)
+    nrm = torch.empty_like(rgb)
+    st = scene._data.settings
+    st = scenes.RenderSettings(size, size, spp, maxBounces=st.maxBounces, russianRouletteDepth=st.russianRouletteDepth,
+                               seed=st.seed, useNEE=st.useNEE)
+    for v, cam in enumerate(cams):
+        renderer.render_device(scene, None, camera=cam, settings=st, d_rgb_ptr=rgb[v].data_ptr(),
+                               d_albedo=_Ptr(alb[v]), d_normal=_Ptr(nrm[v]), sample_offset=sample_offset)
+    return rgb, alb, nrm
+
+
+def generate(scene_seeds, views, size, target_spp, device=0, log=print):
+    """Renders the training set; returns a dict of device tensors."""
+    import torch
+
+    rng = np.random.default_rng(12345)
+    renderer = wrk.Renderer(device=device)
+    tgt, inp = [], {k: ([], [], []) for k in INPUT_SPPS}
+    t0 = time.time()
+    for s in scene_seeds:
+        sd = scenes.scale_test(size, size, 4, seed=s)
+        scene = wrk.Scene.from_data(sd, device)
+        cams = [scenes.Camera(position=sd.camera.position, target=sd.camera.target, up=sd.camera.up,
+                              fovY=sd.camera.fovY, aspect=1.0)]
+        cams += [orbit_camera(rng, size, size) for _ in range(views - 1)]
+        t, _, _ = render_views(scene, renderer, cams, size, target_spp, 0, torch, device)
+        tgt.append(t)
+        off = target_spp
+        for k in INPUT_SPPS:
+            r, a, n = render_views(scene, renderer, cams, size, k, off, torch, device)
+            off += k
+            inp[k][0].append(r)
+            inp[k][1].append(a)
+            inp[k][2].append(n)
+        del scene
+        log(f"scene seed {s}: {len(cams)} views rendered ({time.time() - t0:.1f} s)")
+    data = {"target": torch.cat(tgt)}
+    for k in INPUT_SPPS:
+        data[k] = tuple(torch.cat(x) for x in inp[k])
+    torch.cuda.synchronize()
+    return data
+
+
+def train(data, steps, batch=16, crop=128, lr=1e-3, seed=1, device=0, log=print, dn=None):
+    import torch
+
+    g = torch.Generator(device=f"cuda:{device}")
+    g.manual_seed(seed)
+    dn = dn or wrk.Denoiser(device=device, seed=seed)
+    V, S = data["target"].shape[0], data["target"].shape[1]
+    losses = []
+    t0 = time.time()
+    for it in range(steps):
+        k = INPUT_SPPS[int(torch.randint(len(INPUT_SPPS), (1,), generator=g, device=f"cuda:{device}").item())]
+        vi = torch.randint(V, (batch,), generator=g, device=f"cuda:{device}")
+        oy = torch.randint(S - crop + 1, (batch,), generator=g, device=f"cuda:{device}")
+        ox = torch.randint(S - crop + 1, (batch,), generator=g, device=f"cuda:{device}")
+        ar = torch.arange(crop, device=f"cuda:{device}")
+        yy = (oy[:, None] + ar[None, :])[:, :, None]
+        xx = (ox[:, None] + ar[None, :])[:, None, :]
+        b = vi[:, None, None]
+
+        def take(t):
+            return t[b, yy, xx].contiguous()
+
+        rgb, alb, nrm = (take(t) for t in data[k])
+        tgt = take(data["target"])
+        if it % 2:
+            rgb, alb, nrm, tgt = (t.flip(2).contiguous() for t in (rgb, alb, nrm, tgt))
+            nrm[..., 0] = -nrm[..., 0]
+        cur = lr * (0.1 + 0.9 * 0.5 * (1.0 + math.cos(math.pi * it / max(1, steps))))
+        loss = dn.train_step(_Ptr(rgb), _Ptr(alb), _Ptr(nrm), _Ptr(tgt), batch, crop, crop, cur)
+        losses.append(loss)
+        if it % 250 == 0 or it == steps - 1:
+            log(f"step {it}: loss {np.mean(losses[-50:]):.4f} lr {cur:.2e} ({time.time() - t0:.1f} s)")
+    torch.cuda.synchronize()
+    return dn, losses, time.time() - t0
+
+
+def save_weights(dn: "wrk.Denoiser", path: str, meta: dict) -> None:
+    """Weights as bf16 bit patterns (the precision inference uses) plus metadata."""
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    np.savez_compressed(path, params_bf16=wrk.to_bf16_bits(dn.get_params()), meta=json.dumps(meta))
+
+
+def load_weights(dn: "wrk.Denoiser", path: str = DEFAULT_WEIGHTS) -> dict:
+    z = np.load(path)
+    dn.set_params(wrk.from_bf16_bits(z["params_bf16"]))
+    return json.loads(str(z["meta"]))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--scenes", type=int, default=8)
+    ap.add_argument("--views", type=int, default=16)
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--target-spp", type=int, default=1024)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--log", default=None)
+    args = ap.parse_args()
+    logf = open(args.log, "w") if args.log else None
+
+    def log(msg):
+        print(msg, flush=True)
+        if logf:
+            logf.write(msg + "\n")
+            logf.flush()
+
+    import torch
+
+    t0 = time.time()
+    data = generate(list(range(101, 101 + args.scenes)), args.views, args.size, args.target_spp, log=log)
+    gen_s = time.time() - t0
+    dn, losses, train_s = train(data, args.steps, batch=args.batch, lr=args.lr, log=log)
+    meta = {"scenes": list(range(101, 101 + args.scenes)), "views": args.views, "size": args.size,
+            "target_spp": args.target_spp, "input_spps": list(INPUT_SPPS), "steps": args.steps, "batch": args.batch,
+            "crop": 128, "lr": args.lr, "gen_s": gen_s, "train_s": train_s,
+            "final_loss": float(np.mean(losses[-100:]))}
+    save_weights(dn, args.out, meta)
+    log(json.dumps(meta))
+    del data
+    torch.cuda.empty_cache()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,109 @@
+"""Image-quality measurement: FP64-accumulated references, relMSE, time-to-relMSE.
+
+relMSE(x, r) = mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2), with r
+the FP64-accumulated high-spp reference of the same scene, camera and settings.
+
+time_to_relmse: the plain renderer at `plain_spp` (256 for the scale test) sets
+the quality bar; the denoised renderer searches the smallest spp whose denoised
+image reaches that bar, and the ratio of GPU times (render + denoise vs plain
+render) is the headline of the serving path.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import scenes, wrk
+
+
+class _Ptr:
+    def __init__(self, t):
+        self.t = t
+        self.ptr = t.data_ptr()
+
+
+def relmse(x, ref) -> float:
+    import torch
+
+    if isinstance(x, torch.Tensor):
+        x64 = x.double()
+        r64 = ref.double()
+        return float(torch.mean((x64 - r64) ** 2 / (r64 * r64 + 1e-2)).item())
+    x = np.asarray(x, np.float64)
+    r = np.asarray(ref, np.float64)
+    return float(np.mean((x - r) ** 2 / (r * r + 1e-2)))
+
+
+def _settings(st, spp):
+    return scenes.RenderSettings(st.width, st.height, spp, maxBounces=st.maxBounces,
+                                 russianRouletteDepth=st.russianRouletteDepth, useNEE=st.useNEE,
+                                 fireflyClamp=st.fireflyClamp, seed=st.seed)
+
+
+def render(renderer, scene, cam, st, spp, sample_offset, torch, device=0, guides=True):
+    """(rgb, albedo, normal) device tensors (H, W, 3) of one render; gpu ms."""
+    H, W = st.height, st.width
+    rgb = torch.empty((H, W, 3), dtype=torch.float32, device=f"cuda:{device}")
+    alb = torch.empty_like(rgb) if guides else None
+    nrm = torch.empty_like(rgb) if guides else None
+    s = renderer.render_device(scene, None, camera=cam, settings=_settings(st, spp), d_rgb_ptr=rgb.data_ptr(),
+                               d_albedo=_Ptr(alb) if guides else None, d_normal=_Ptr(nrm) if guides else None,
+                               sample_offset=sample_offset)
+    return rgb, alb, nrm, s["gpuMs"]
+
+
+def reference(renderer, scene, cam, st, total_spp=4096, chunk=256, sample_offset=1 << 20, device=0):
+    """FP64-accumulated reference: chunks of `chunk` spp (f32 per-pixel sums inside a
+    chunk) summed in float64 over disjoint sample ranges."""
+    import torch
+
+    acc = torch.zeros((st.height, st.width, 3), dtype=torch.float64, device=f"cuda:{device}")
+    n = 0
+    while n < total_spp:
+        k = min(chunk, total_spp - n)
+        rgb, _, _, _ = render(renderer, scene, cam, st, k, sample_offset + n, torch, device, guides=False)
+        acc += rgb.double() * k
+        n += k
+    return acc / total_spp
+
+
+def time_to_relmse(renderer, denoiser, scene, cam, st, ref, plain_spp=256, search=(1, 2, 4, 8, 16, 32, 64, 128),
+                   device=0, repeats=2):
+    """Plain render at plain_spp vs render+denoise at increasing spp until the
+    denoised relMSE reaches the plain one.  Times are device times (CUDA events)."""
+    import torch
+
+    def timed(fn):
+        best = None
+        out = None
+        for _ in range(repeats):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            out = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        return out, best
+
+    H, W = st.height, st.width
+    (plain, _, _, _), plain_ms = timed(lambda: render(renderer, scene, cam, st, plain_spp, 0, torch, device, False))
+    bar = relmse(plain, ref)
+    rows = []
+    found = None
+    for s in search:
+        def run():
+            rgb, alb, nrm, _ = render(renderer, scene, cam, st, s, 0, torch, device, True)
+            out = torch.empty_like(rgb)
+            denoiser.infer_device(_Ptr(rgb), _Ptr(alb), _Ptr(nrm), 1, H, W, _Ptr(out))
+            return rgb, out
+
+        (noisy, den), ms = timed(run)
+        r = {"spp": s, "ms": ms, "relmse_noisy": relmse(noisy, ref), "relmse_denoised": relmse(den, ref)}
+        rows.append(r)
+        if found is None and r["relmse_denoised"] <= bar:
+            found = r
+            break
+    return {"plain_spp": plain_spp, "plain_ms": plain_ms, "plain_relmse": bar, "search": rows,
+            "denoised_spp": found["spp"] if found else None, "denoised_ms": found["ms"] if found else None,
+            "time_ratio": (found["ms"] / plain_ms) if found else None}

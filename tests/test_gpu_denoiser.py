@@ -140,3 +140,27 @@ def test_denoiser_training_lowers_loss_and_pads(gpu):
     # arbitrary sizes are padded internally; output keeps the input's shape
     small = dn.infer(rgb[0, :37, :53], alb[0, :37, :53], nrm[0, :37, :53])
     assert small.shape == (37, 53, 3) and np.isfinite(small).all() and (small >= 0).all()
+
+
+def test_trained_denoiser_gains_on_held_out_scene(gpu):
+    """The committed weights (trained by offlinerenderer_b200.denoise_train on scene
+    seeds 101-108) on the held-out benchmark scene (scale test, seed 1): the
+    denoised 4-spp image is far closer to an FP64-accumulated 1024-spp reference
+    than the 4-spp render it came from, and closer than the plain 64-spp render."""
+    import torch
+
+    from offlinerenderer_b200 import denoise_train, quality, scenes
+
+    sd = scenes.scale_test(256, 256, 4, seed=1)
+    scene = gpu.Scene.from_data(sd)
+    renderer = gpu.Renderer()
+    st, cam = sd.settings, sd.camera
+    ref = quality.reference(renderer, scene, cam, st, total_spp=1024, chunk=256)
+    dn = gpu.Denoiser()
+    denoise_train.load_weights(dn, denoise_train.DEFAULT_WEIGHTS)
+    rgb, alb, nrm, _ = quality.render(renderer, scene, cam, st, 4, 0, torch)
+    out = torch.empty_like(rgb)
+    dn.infer_device(quality._Ptr(rgb), quality._Ptr(alb), quality._Ptr(nrm), 1, 256, 256, quality._Ptr(out))
+    plain64, _, _, _ = quality.render(renderer, scene, cam, st, 64, 4, torch, guides=False)
+    noisy, den, p64 = quality.relmse(rgb, ref), quality.relmse(out, ref), quality.relmse(plain64, ref)
+    assert den < 0.1 * noisy and den < p64, (noisy, den, p64)
