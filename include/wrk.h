@@ -69,6 +69,8 @@ typedef struct {
 /* Record CUDA events around every kernel of the loop (on the renderer's stream)
  * and report per-stage device time in wrk_render_stats.stageMs. */
 #define WRK_FLAG_STAGE_TIMING 2u
+/* Served requests: pass the result through the server's learned denoiser. */
+#define WRK_FLAG_DENOISE 4u
 
 enum {
     WRK_STAGE_CONTROL = 0,
@@ -158,6 +160,10 @@ int wrk_scene_buffers_get(wrk_scene* s, wrk_scene_buffers* out);
 /* capacity = path slots in flight (0 = chosen from the device). */
 int wrk_renderer_create(int device, uint32_t capacity, wrk_renderer** out);
 int wrk_renderer_destroy(wrk_renderer* r);
+/* Launch shape of the bounce loop: iterations per captured CUDA graph launch
+ * (1..64, default 8) and threads per shading block (128 or 256, default 256);
+ * wrk_autotune picks them. */
+int wrk_renderer_set_launch(wrk_renderer* r, uint32_t chunk, uint32_t shadeBlock);
 /* Synchronous render into HOST buffers of width*height*3 floats: rgb = sum/spp
  * (renderer.cpp:308-313), albedo / normal first-hit guides (may be NULL). */
 int wrk_render(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, const wrk_render_params* p, float* rgb,
@@ -166,6 +172,70 @@ int wrk_render(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, const wrk_r
  * stream; the call returns after the loop has finished on the device. */
 int wrk_render_device(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, const wrk_render_params* p, float* d_rgb,
                       float* d_albedo, float* d_normal, wrk_render_stats* stats);
+
+/* ---- serving loop: no counterpart in libWR, which renders one image per
+ *      synchronous Renderer::render call (libWR/src/internal/renderer.cpp:132-316) ----
+ * A server keeps scenes resident and renders many requests (any size, spp, camera,
+ * scene) at once: admitted requests share one set of wavefront queues, new ones
+ * join while others are in flight (admission by free slot and by room in an
+ * accumulation pool of poolBytes, first come first served), and each step runs one
+ * captured CUDA graph of `chunk` bounce iterations for all of them.  A request's
+ * image is the same alone and in the mix (RNG keyed by seed, pixel and sample)
+ * up to the order of f32 sums.  Scenes must outlive the server. */
+typedef struct wrk_server wrk_server;
+typedef struct wrk_denoiser wrk_denoiser;
+typedef struct {
+    uint32_t capacity;     /* path entries in flight (0 = 4M) */
+    uint32_t maxRequests;  /* concurrent requests (0 or > 64 = 64) */
+    uint64_t poolBytes;    /* HBM for per-request buffers, 96 bytes per pixel (0 = 4 GiB) */
+    uint32_t chunk;        /* bounce iterations per step (0 = 8) */
+    uint32_t shadeBlock;   /* 128 or 256 (0 = 256) */
+} wrk_server_config;
+typedef struct {
+    uint32_t queued, running, ready;
+    uint64_t iterations;   /* bounce iterations run so far */
+    float lastChunkMs;     /* device time of the last step's chunk */
+    uint64_t poolFreeBytes;
+} wrk_server_status;
+typedef struct {
+    uint32_t width, height, spp, denoised;
+    double submitMs, admitMs, readyMs; /* host clock, ms since the server was created */
+    uint32_t iterations;               /* bounce iterations from admission to completion */
+} wrk_request_info;
+int wrk_server_create(int device, const wrk_server_config* cfg, wrk_server** out);
+int wrk_server_destroy(wrk_server* s);
+/* Requests flagged WRK_FLAG_DENOISE are passed through this denoiser. */
+int wrk_server_set_denoiser(wrk_server* s, wrk_denoiser* d);
+int wrk_server_submit(wrk_server* s, wrk_scene* scene, const wrk_camera* cam, const wrk_render_params* p,
+                      uint64_t* ticket);
+/* Admits, runs one chunk for every request in flight, retires finished ones. */
+int wrk_server_step(wrk_server* s, wrk_server_status* status);
+int wrk_server_poll(wrk_server* s, uint64_t ticket, int* ready);
+/* Steps until the request is ready. */
+int wrk_server_wait(wrk_server* s, uint64_t ticket);
+/* Copies a ready request's images (width*height*3 floats each; rgb is the denoised
+ * image when the request asked for it; albedo / normal may be NULL) to host memory
+ * (or device memory: _device) and releases the request. */
+int wrk_server_result(wrk_server* s, uint64_t ticket, float* rgb, float* albedo, float* normal,
+                      wrk_request_info* info);
+int wrk_server_result_device(wrk_server* s, uint64_t ticket, float* d_rgb, float* d_albedo, float* d_normal,
+                             wrk_request_info* info);
+
+/* ---- autotuner: no counterpart in libWR.  Times one render of the given
+ *      workload per launch shape (capacity 1M/2M/4M x chunk 4/8/16 x shading
+ *      block 128/256) and returns the fastest. ---- */
+typedef struct {
+    uint32_t capacity, chunk, shadeBlock;
+    float ms;
+} wrk_tune_trial;
+typedef struct {
+    uint32_t capacity, chunk, shadeBlock;
+    float bestMs;
+    uint32_t numTrials;
+    wrk_tune_trial trials[32];
+} wrk_tune_result;
+int wrk_autotune(int device, wrk_scene* scene, const wrk_camera* cam, const wrk_render_params* p,
+                 wrk_tune_result* out);
 
 /* ---- kernel-level entry points (device pointers; synchronous) ---- */
 /* Closest hit (optixTrace + __closesthit__trace, trace.cu:127-141):
@@ -219,7 +289,6 @@ int wrk_conv3x3_forward(const void* d_x, uint32_t B, uint32_t H, uint32_t W, uin
 int wrk_conv3x3_wgrad(const void* d_g, const void* d_x, uint32_t B, uint32_t H, uint32_t W, uint32_t Cin,
                       uint32_t Cout, float* d_dw);
 
-typedef struct wrk_denoiser wrk_denoiser;
 /* A 4-level U-Net (32/64/128/256 channels) on radiance + albedo + normal, weights
  * initialised from `seed`.  Parameters are one f32 array: per layer W [Cout][3][3][Cin]
  * then bias [Cout], layers in the order e0a e0b e1a e1b e2a e2b e3a e3b d2a d2b d1a

@@ -24,7 +24,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 # The system g++ (an exported CXX may be a wrapper without the C++20 headers needed here).
 CXX = "g++"
 
-CU_SOURCES = ["bvh_build.cu", "trace.cu", "render.cu", "kernels_misc.cu", "api.cu", "conv_tc.cu", "denoiser.cu"]
+CU_SOURCES = ["bvh_build.cu", "trace.cu", "render.cu", "kernels_misc.cu", "api.cu", "conv_tc.cu", "denoiser.cu", "server.cu"]
 CPP_SOURCES = ["wr_api.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off",

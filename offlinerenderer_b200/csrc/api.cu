@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "engine.h"
 #include "wrk_internal.h"
 
 namespace wrk {
@@ -134,26 +135,190 @@ struct wrk_scene {
     }
 };
 
+namespace wrk {
+// Accessors other translation units use (the scene's layout stays private here).
+const DevScene* scene_view(const wrk_scene* s) { return s && s->finalized ? &s->view : nullptr; }
+int scene_device(const wrk_scene* s) { return s ? s->device : -1; }
+}  // namespace wrk
+
 struct wrk_renderer {
-    int device = 0;
-    uint32_t capacity = 0;
-    int numSMs = 148;
-    cudaStream_t stream = nullptr;
+    Engine eng;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evLoop0 = nullptr, evLoop1 = nullptr;
-    std::vector<cudaEvent_t> stageEv;  // per-launch events for WRK_FLAG_STAGE_TIMING
-    DevBuf queues, counters, frameBufs, outBufs;
-    Counters* hostCtr = nullptr;  // pinned
-    Queues q{};
+    DevBuf frameBufs, outBufs;
     ~wrk_renderer() {
-        if (hostCtr) cudaFreeHost(hostCtr);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (evLoop0) cudaEventDestroy(evLoop0);
         if (evLoop1) cudaEventDestroy(evLoop1);
-        for (cudaEvent_t e : stageEv) cudaEventDestroy(e);
-        if (stream) cudaStreamDestroy(stream);
     }
 };
+
+// ---------------------------------------------------------------------------
+// Engine
+namespace wrk {
+
+Engine::~Engine() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (graph) cudaGraphExecDestroy(graph);
+    for (cudaEvent_t e : stageEv) cudaEventDestroy(e);
+    if (hCtr) cudaFreeHost(hCtr);
+    if (hCtl) cudaFreeHost(hCtl);
+    if (hReq) cudaFreeHost(hReq);
+    if (hGenOrder) cudaFreeHost(hGenOrder);
+    if (hScenes) cudaFreeHost(hScenes);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+cudaError_t Engine::init(int dev, uint32_t cap) {
+    device = dev;
+    cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, dev);
+    capacity = std::max(cap ? cap : (1u << 22), 1024u);
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    if ((e = cudaMallocHost(&hCtr, sizeof(Counters))) != cudaSuccess ||
+        (e = cudaMallocHost(&hCtl, sizeof(SlotCtl) * kMaxSlots)) != cudaSuccess ||
+        (e = cudaMallocHost(&hReq, sizeof(Frame) * kMaxSlots)) != cudaSuccess ||
+        (e = cudaMallocHost(&hGenOrder, sizeof(uint32_t) * (kMaxSlots + 4))) != cudaSuccess ||
+        (e = cudaMallocHost(&hScenes, sizeof(DevScene) * kMaxScenes)) != cudaSuccess)
+        return e;
+    memset(hCtl, 0, sizeof(SlotCtl) * kMaxSlots);
+    memset(hGenOrder, 0, sizeof(uint32_t) * (kMaxSlots + 4));
+    // SoA path queues: extension x2 (5 fields), shadow x2 (9 fields), buckets (6 fields)
+    size_t C = capacity;
+    const size_t fields = 2 * 5 + 2 * 9 + kNumBuckets * 6;
+    if ((e = queues.alloc(C * fields * sizeof(float4))) != cudaSuccess) return e;
+    float4* next = queues.as<float4>();
+    auto take = [&]() {
+        float4* p = next;
+        next += C;
+        return p;
+    };
+    for (int k = 0; k < 2; ++k) {
+        PathQ& x = q.ext[k];
+        x = PathQ{};
+        x.ray_o = take();
+        x.ray_d = take();
+        x.thr = take();
+        x.rad = take();
+        x.st = reinterpret_cast<uint4*>(take());
+        PathQ& h = q.shd[k];
+        h = PathQ{};
+        h.ray_o = take();
+        h.ray_d = take();
+        h.hit = take();
+        h.thr = take();
+        h.rad = take();
+        h.st = reinterpret_cast<uint4*>(take());
+        h.sh_o = take();
+        h.sh_d = take();
+        h.sh_c = take();
+    }
+    for (int b = 0; b < kNumBuckets; ++b) {
+        PathQ& x = q.bucket[b];
+        x = PathQ{};
+        x.ray_o = take();
+        x.ray_d = take();
+        x.hit = take();
+        x.thr = take();
+        x.rad = take();
+        x.st = reinterpret_cast<uint4*>(take());
+    }
+    if ((e = counters.alloc(sizeof(Counters))) != cudaSuccess) return e;
+    // tables: requests | slot progress | scenes | admission order | generation segments
+    auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t oReq = 0, oCtl = oReq + up(sizeof(Frame) * kMaxSlots), oSc = oCtl + up(sizeof(SlotCtl) * kMaxSlots),
+                 oGo = oSc + up(sizeof(DevScene) * kMaxScenes), oSeg = oGo + up(sizeof(uint32_t) * (kMaxSlots + 4)),
+                 total = oSeg + up(sizeof(GenSeg) * kMaxSlots);
+    if ((e = tables.alloc(total)) != cudaSuccess) return e;
+    if ((e = cudaMemset(tables.p, 0, total)) != cudaSuccess) return e;
+    uint8_t* t = tables.as<uint8_t>();
+    dReq = reinterpret_cast<Frame*>(t + oReq);
+    dCtl = reinterpret_cast<SlotCtl*>(t + oCtl);
+    dScenes = reinterpret_cast<DevScene*>(t + oSc);
+    dGenOrder = reinterpret_cast<uint32_t*>(t + oGo);
+    dSeg = reinterpret_cast<GenSeg*>(t + oSeg);
+    q.ctr = counters.as<Counters>();
+    q.capacity = capacity;
+    q.req = dReq;
+    q.ctl = dCtl;
+    q.scenes = dScenes;
+    q.genOrder = dGenOrder;
+    q.seg = dSeg;
+    return reset_counters();
+}
+
+cudaError_t Engine::reset_counters() {
+    cudaError_t e = cudaMemsetAsync(q.ctr, 0, sizeof(Counters), stream);
+    if (e != cudaSuccess) return e;
+    hGenOrder[kMaxSlots + 3] = 1;  // staging word for Counters::cur (the control kernel swaps first)
+    return cudaMemcpyAsync(&q.ctr->cur, &hGenOrder[kMaxSlots + 3], sizeof(uint32_t), cudaMemcpyHostToDevice, stream);
+}
+
+static void launch_iteration(const Engine& E, const DevScene& s0, bool multi, cudaStream_t st, cudaEvent_t* ev) {
+    if (ev) cudaEventRecord(ev[0], st);
+    launch_control(E.q, st);
+    if (ev) cudaEventRecord(ev[1], st);
+    launch_generate(E.q, E.numSMs * 8, st);
+    if (ev) cudaEventRecord(ev[2], st);
+    launch_trace_extension(s0, E.q, multi, E.trace_grid(), st);
+    if (ev) cudaEventRecord(ev[3], st);
+    launch_trace_shadow(s0, E.q, multi, E.trace_grid(), st);
+    if (ev) cudaEventRecord(ev[4], st);
+    for (uint32_t b = 0; b < kNumBuckets; ++b) {
+        launch_shade_bucket(b, s0, E.q, multi, E.shade_grid(), (int)E.cfg.shadeBlock, st);
+        if (ev) cudaEventRecord(ev[5 + b], st);
+    }
+}
+
+cudaError_t Engine::enqueue_chunk(const DevScene& s0, bool multi, bool timing) {
+    cudaError_t e;
+    if (timing) {
+        while (stageEv.size() < cfg.chunk * 10) {
+            cudaEvent_t ev;
+            if ((e = cudaEventCreate(&ev)) != cudaSuccess) return e;
+            stageEv.push_back(ev);
+        }
+        for (uint32_t k = 0; k < cfg.chunk; ++k) launch_iteration(*this, s0, multi, stream, &stageEv[k * 10]);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    } else {
+        const bool same = graph && multi == graphMulti && memcmp(&s0, &graphScene, sizeof(DevScene)) == 0 &&
+                          graphCfg.chunk == cfg.chunk && graphCfg.shadeBlock == cfg.shadeBlock &&
+                          graphCfg.traceBlocksPerSM == cfg.traceBlocksPerSM &&
+                          graphCfg.shadeBlocksPerSM == cfg.shadeBlocksPerSM;
+        if (!same) {
+            if (graph) cudaGraphExecDestroy(graph);
+            graph = nullptr;
+            if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+            for (uint32_t k = 0; k < cfg.chunk; ++k) launch_iteration(*this, s0, multi, stream, nullptr);
+            cudaGraph_t g = nullptr;
+            e = cudaStreamEndCapture(stream, &g);
+            if (e != cudaSuccess) return e;
+            e = cudaGraphInstantiate(&graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return e;
+            graphMulti = multi;
+            memcpy(&graphScene, &s0, sizeof(DevScene));
+            graphCfg = cfg;
+        }
+        if ((e = cudaGraphLaunch(graph, stream)) != cudaSuccess) return e;
+    }
+    if ((e = cudaMemcpyAsync(hCtr, q.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, stream)) != cudaSuccess) return e;
+    return cudaMemcpyAsync(hCtl, dCtl, sizeof(SlotCtl) * kMaxSlots, cudaMemcpyDeviceToHost, stream);
+}
+
+cudaError_t Engine::stage_times(float* ms, uint32_t* launches) {
+    for (uint32_t k = 0; k < cfg.chunk; ++k)
+        for (int j = 0; j < WRK_NUM_STAGES; ++j) {
+            float t = 0;
+            cudaError_t e = cudaEventElapsedTime(&t, stageEv[k * 10 + j], stageEv[k * 10 + j + 1]);
+            if (e != cudaSuccess) return e;
+            ms[j] += t;
+            launches[j] += 1;
+        }
+    return cudaSuccess;
+}
+
+}  // namespace wrk
 
 namespace {
 
@@ -417,159 +582,104 @@ int wrk_renderer_create(int device, uint32_t capacity, wrk_renderer** out) {
     int rc = set_device(device);
     if (rc) return rc;
     wrk_renderer* r = new wrk_renderer();
-    r->device = device;
-    cudaDeviceGetAttribute(&r->numSMs, cudaDevAttrMultiProcessorCount, device);
-    if (capacity == 0) capacity = 1u << 22;
-    capacity = std::max(capacity, 1024u);
-    r->capacity = capacity;
-    auto bail = [&](int code) {
+    cudaError_t e = r->eng.init(device, capacity);
+    if (e == cudaSuccess && (cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess ||
+                             cudaEventCreate(&r->evLoop0) != cudaSuccess || cudaEventCreate(&r->evLoop1) != cudaSuccess))
+        e = cudaErrorUnknown;
+    if (e != cudaSuccess) {
         delete r;
-        return code;
-    };
-    if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess ||
-        cudaEventCreate(&r->evLoop0) != cudaSuccess || cudaEventCreate(&r->evLoop1) != cudaSuccess)
-        return bail(fail(WRK_ERR_CUDA, "stream/event creation failed"));
-    if (cudaMallocHost(&r->hostCtr, sizeof(Counters)) != cudaSuccess)
-        return bail(fail(WRK_ERR_CUDA, "pinned counter allocation failed"));
-    // SoA path queues: extension x2 (5 fields), shadow x2 (9 fields), buckets (6 fields)
-    size_t C = capacity;
-    const size_t fields = 2 * 5 + 2 * 9 + kNumBuckets * 6;
-    if ((rc = r->queues.alloc(C * fields * sizeof(float4)))) return bail(rc);
-    float4* next = r->queues.as<float4>();
-    auto take = [&]() {
-        float4* p = next;
-        next += C;
-        return p;
-    };
-    for (int k = 0; k < 2; ++k) {
-        PathQ& e = r->q.ext[k];
-        e = PathQ{};
-        e.ray_o = take();
-        e.ray_d = take();
-        e.thr = take();
-        e.rad = take();
-        e.st = reinterpret_cast<uint4*>(take());
-        PathQ& h = r->q.shd[k];
-        h = PathQ{};
-        h.ray_o = take();
-        h.ray_d = take();
-        h.hit = take();
-        h.thr = take();
-        h.rad = take();
-        h.st = reinterpret_cast<uint4*>(take());
-        h.sh_o = take();
-        h.sh_d = take();
-        h.sh_c = take();
+        return fail(WRK_ERR_CUDA, "renderer creation failed: %s", cudaGetErrorString(e));
     }
-    for (int b = 0; b < kNumBuckets; ++b) {
-        PathQ& e = r->q.bucket[b];
-        e = PathQ{};
-        e.ray_o = take();
-        e.ray_d = take();
-        e.hit = take();
-        e.thr = take();
-        e.rad = take();
-        e.st = reinterpret_cast<uint4*>(take());
-    }
-    if ((rc = r->counters.alloc(sizeof(Counters)))) return bail(rc);
-    r->q.ctr = r->counters.as<Counters>();
-    r->q.capacity = capacity;
     *out = r;
     return WRK_OK;
 }
 
 int wrk_renderer_destroy(wrk_renderer* r) {
     if (r) {
-        cudaSetDevice(r->device);
-        cudaStreamSynchronize(r->stream);
+        cudaSetDevice(r->eng.device);
         delete r;
     }
     return WRK_OK;
 }
 
+int wrk_renderer_set_launch(wrk_renderer* r, uint32_t chunk, uint32_t shadeBlock) {
+    if (!r) return fail(WRK_ERR_INVALID, "null renderer");
+    if (chunk < 1 || chunk > 64 || (shadeBlock != 128 && shadeBlock != 256))
+        return fail(WRK_ERR_INVALID, "chunk must be 1..64 and shadeBlock 128 or 256");
+    r->eng.cfg.chunk = chunk;
+    r->eng.cfg.shadeBlock = shadeBlock;
+    return WRK_OK;
+}
+
+}  // extern "C"
+
+namespace wrk {
+// The request record the kernels read for one render (camera basis as libWR
+// computes it, settings, sums).
+void fill_frame(Frame& f, const wrk_camera& cam, const wrk_render_params& p) {
+    f = Frame{};
+    camera_frame(cam, f);
+    f.width = p.width;
+    f.height = p.height;
+    f.spp = p.spp;
+    f.useNEE = p.useNEE ? 1u : 0u;
+    f.maxBounces = p.maxBounces;
+    f.seed = p.seed;
+    f.sampleOffset = p.sampleOffset;
+    f.maxIter = p.maxIterations ? p.maxIterations : 8u;
+    f.rrStart = p.russianRouletteDepth;
+    f.fireflyClamp = p.fireflyClamp;
+    f.tilesX = (p.width % 8 == 0 && p.height % 4 == 0) ? p.width / 8 : 0;
+    f.perSample = p.width * p.height;
+}
+}  // namespace wrk
+
+extern "C" {
+
 static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, const wrk_render_params* p, float* d_rgb,
                        float* d_alb, float* d_nrm, wrk_render_stats* stats) {
-    Frame f{};
-    camera_frame(*cam, f);
-    f.width = p->width;
-    f.height = p->height;
-    f.spp = p->spp;
-    f.useNEE = p->useNEE ? 1u : 0u;
-    f.maxBounces = p->maxBounces;
-    f.seed = p->seed;
-    f.sampleOffset = p->sampleOffset;
-    f.maxIter = p->maxIterations ? p->maxIterations : 8u;
-    f.rrStart = p->russianRouletteDepth;
-    f.fireflyClamp = p->fireflyClamp;
-    f.tilesX = (p->width % 8 == 0 && p->height % 4 == 0) ? p->width / 8 : 0;
-    f.perSample = p->width * p->height;
+    Engine& E = r->eng;
+    Frame f;
+    fill_frame(f, *cam, *p);
     size_t np = (size_t)p->width * p->height;
     int rc = r->frameBufs.alloc(np * 3 * sizeof(float4));
     if (rc) return rc;
     f.accum = r->frameBufs.as<float4>();
     f.albedo = f.accum + np;
     f.normal = f.albedo + np;
-    f.err = &r->q.ctr->error;
-    cudaStream_t st = r->stream;
+    f.err = &E.q.ctr->error;
+    f.scene = 0;
+    cudaStream_t st = E.stream;
     CK(cudaEventRecord(r->ev0, st));
     CK(cudaMemsetAsync(f.accum, 0, np * 3 * sizeof(float4), st));
-    Counters c0{};
-    c0.cur = 1;
-    c0.totalWork = (unsigned long long)np * p->spp;
-    CK(cudaMemcpyAsync(r->q.ctr, &c0, sizeof(Counters), cudaMemcpyHostToDevice, st));
-    const int traceGrid = r->numSMs * 8, shadeGrid = r->numSMs * 4;
+    E.hReq[0] = f;
+    E.hScenes[0] = s->view;
+    SlotCtl sc{};
+    sc.workTotal = (unsigned long long)np * p->spp;
+    sc.state = kSlotActive;
+    E.hCtl[0] = sc;
+    E.hGenOrder[0] = 1;
+    E.hGenOrder[1] = 0;
+    CK(cudaMemcpyAsync(E.dReq, E.hReq, sizeof(Frame), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(E.dScenes, E.hScenes, sizeof(DevScene), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(E.dCtl, E.hCtl, sizeof(SlotCtl), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(E.dGenOrder, E.hGenOrder, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CK(E.reset_counters());
     // bound on iterations: every path needs <= maxIter; waves of `capacity` paths
-    unsigned long long waves = c0.totalWork / r->capacity + 2;
+    unsigned long long waves = sc.workTotal / E.capacity + 2;
     unsigned long long maxIters = waves * (unsigned long long)(f.maxIter + 2) * 4ull + 64ull;
     uint32_t iters = 0;
-    const uint32_t kChunk = 8;
     const bool timing = (p->flags & WRK_FLAG_STAGE_TIMING) != 0;
-    // one event before and after each of the 9 launches of an iteration
-    if (timing && r->stageEv.size() < kChunk * 10) {
-        while (r->stageEv.size() < kChunk * 10) {
-            cudaEvent_t e;
-            CK(cudaEventCreate(&e));
-            r->stageEv.push_back(e);
-        }
-    }
     float stageMs[WRK_NUM_STAGES] = {0};
     uint32_t stageN[WRK_NUM_STAGES] = {0};
     CK(cudaEventRecord(r->evLoop0, st));
     while (true) {
-        for (uint32_t k = 0; k < kChunk; ++k) {
-            cudaEvent_t* ev = timing ? &r->stageEv[k * 10] : nullptr;
-            if (timing) CK(cudaEventRecord(ev[0], st));
-            launch_control(r->q, st);
-            if (timing) CK(cudaEventRecord(ev[1], st));
-            launch_generate(r->q, f, r->numSMs * 8, st);
-            if (timing) CK(cudaEventRecord(ev[2], st));
-            launch_trace_extension(s->view, r->q, f, traceGrid, st);
-            if (timing) CK(cudaEventRecord(ev[3], st));
-            launch_trace_shadow(s->view, r->q, f, traceGrid, st);
-            if (timing) CK(cudaEventRecord(ev[4], st));
-            for (uint32_t b = 0; b < kNumBuckets; ++b) {
-                launch_shade_bucket(b, s->view, r->q, f, shadeGrid, st);
-                if (timing) CK(cudaEventRecord(ev[5 + b], st));
-            }
-        }
-        iters += kChunk;
-        CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(r->hostCtr, r->q.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+        CK(E.enqueue_chunk(s->view, false, timing));
+        iters += E.cfg.chunk;
         CK(cudaStreamSynchronize(st));
-        if (timing) {
-            for (uint32_t k = 0; k < kChunk; ++k)
-                for (int j = 0; j < WRK_NUM_STAGES; ++j) {
-                    float ms = 0;
-                    CK(cudaEventElapsedTime(&ms, r->stageEv[k * 10 + j], r->stageEv[k * 10 + j + 1]));
-                    stageMs[j] += ms;
-                    stageN[j] += 1;
-                }
-        }
-        const Counters& h = *r->hostCtr;
-        uint32_t out = h.cur ^ 1u;
-        if (h.error) return fail(WRK_ERR_DEVICE, "device error flags 0x%x during render", h.error);
-        if (h.nextWork == h.totalWork && h.ext[out].v == 0 && h.shd[out].v == 0) break;
+        if (timing) CK(E.stage_times(stageMs, stageN));
+        if (E.hCtr->error) return fail(WRK_ERR_DEVICE, "device error flags 0x%x during render", E.hCtr->error);
+        if (E.hCtl[0].state == kSlotDone) break;
         if (iters > maxIters) return fail(WRK_ERR_DEVICE, "render did not converge after %u iterations", iters);
     }
     CK(cudaEventRecord(r->evLoop1, st));
@@ -578,9 +688,8 @@ static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, con
     CK(cudaEventRecord(r->ev1, st));
     CK(cudaEventSynchronize(r->ev1));
     if (stats) {
-        const Counters& h = *r->hostCtr;
+        const Counters& h = *E.hCtr;
         stats->paths = h.paths;
-        // the last iteration's queues were never folded in by a following control step
         stats->extensionRays = h.extRays;
         stats->shadowRays = h.shdRays;
         for (int b = 0; b < kNumBuckets; ++b) stats->bucketPaths[b] = h.bucketTotal[b] + h.bucket[b].v;
@@ -600,7 +709,7 @@ static int check_render_args(wrk_renderer* r, wrk_scene* s, const wrk_camera* ca
     if (!r || !cam || !p) return fail(WRK_ERR_INVALID, "null renderer/camera/params");
     int rc = check_scene(s);
     if (rc) return rc;
-    if (s->device != r->device) return fail(WRK_ERR_INVALID, "scene and renderer on different devices");
+    if (s->device != r->eng.device) return fail(WRK_ERR_INVALID, "scene and renderer on different devices");
     if (p->width == 0 || p->height == 0 || p->spp == 0) return fail(WRK_ERR_INVALID, "empty render (w/h/spp = 0)");
     if ((uint64_t)p->width * p->height > (1ull << 31)) return fail(WRK_ERR_INVALID, "image too large");
     return WRK_OK;

@@ -43,9 +43,27 @@ __device__ __forceinline__ uint32_t append_pos(uint32_t* counter, bool pred, uin
     return pred ? pos : kInvalidSlot;
 }
 
+// Paths that ended in this warp, counted per request slot with one atomic per
+// distinct slot (warp-aggregated with __match_any_sync).  All lanes call it.
+__device__ __forceinline__ void count_ended(SlotCtl* ctl, bool ended, uint32_t slot) {
+    const uint32_t m = __ballot_sync(0xffffffffu, ended);
+    if (!m) return;
+    const uint32_t peers = __match_any_sync(0xffffffffu, ended ? slot : 0xffffffffu) & m;
+    if (ended && (uint32_t)(__ffs(peers) - 1) == (threadIdx.x & 31u))
+        atomicAdd(&ctl[slot].finished, (unsigned long long)__popc(peers));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// One thread: folds the last iteration's statistics, swaps the queue buffers,
+// marks finished requests done, and hands the room the live paths leave to the
+// active requests' remaining work items in admission (FIFO) order.
 __global__ void k_control(Queues q) {
     Counters* c = q.ctr;
-    // statistics of the iteration that just finished
     for (int b = 0; b < kNumBuckets; ++b) c->bucketTotal[b] += c->bucket[b].v;
     uint32_t cur = c->cur ^ 1u;
     uint32_t out = cur ^ 1u;
@@ -61,11 +79,33 @@ __global__ void k_control(Queues q) {
         c->error |= kErrQueueOverflow;
         live = q.capacity;
     }
-    unsigned long long remaining = c->totalWork - c->nextWork;
-    uint32_t g = (uint32_t)min((unsigned long long)(q.capacity - live), remaining);
+    unsigned long long room = q.capacity - live;
+    const uint32_t n = min(q.genOrder[0], kMaxSlots);
+    uint32_t g = 0, ns = 0, active = 0;
+    const unsigned long long now = global_ns();
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t slot = q.genOrder[1 + k];
+        if (slot >= kMaxSlots) continue;
+        SlotCtl& sc = q.ctl[slot];
+        if (sc.state != kSlotActive) continue;
+        if (sc.workNext >= sc.workTotal && sc.finished >= sc.workTotal) {
+            sc.state = kSlotDone;
+            sc.doneNs = now;
+            sc.doneIter = c->iteration;
+            continue;
+        }
+        ++active;
+        const unsigned long long take = min(sc.workTotal - sc.workNext, room);
+        if (take == 0) continue;
+        q.seg[ns] = GenSeg{sc.workNext, slot, (uint32_t)take, g, 0u};
+        ++ns;
+        sc.workNext += take;
+        room -= take;
+        g += (uint32_t)take;
+    }
+    c->activeSlots = active;
+    c->numSeg = ns;
     c->genCount = g;
-    c->genWorkBase = c->nextWork;
-    c->nextWork += g;
     c->genExtBase = c->ext[cur].v;
     c->ext[cur].v += g;
     c->paths += g;
@@ -76,47 +116,61 @@ __global__ void k_control(Queues q) {
 
 void launch_control(const Queues& q, cudaStream_t st) { k_control<<<1, 1, 0, st>>>(q); }
 
-// Camera ray for (pixel, sample): trace.cu:54-125.
-__global__ void __launch_bounds__(kShadeBlock) k_generate(Queues q, Frame f) {
+// Camera ray for (pixel, sample) of the request a work item belongs to: trace.cu:54-125.
+__global__ void __launch_bounds__(kShadeBlock) k_generate(Queues q) {
+    __shared__ GenSeg seg[kMaxSlots];
     Counters* c = q.ctr;
     const uint32_t g = c->genCount;
     const uint32_t eb = c->genExtBase;
+    const uint32_t ns = min(c->numSeg, kMaxSlots);
+    for (uint32_t k = threadIdx.x; k < ns; k += blockDim.x) seg[k] = q.seg[k];
+    __syncthreads();
     const PathQ o = c->cur ? q.ext[1] : q.ext[0];
-    const unsigned long long wb = c->genWorkBase;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g; i += gridDim.x * blockDim.x) {
-        const uint32_t e = eb + i;
-        unsigned long long w = wb + i;
-        uint32_t sample = f.sampleOffset + (uint32_t)(w / f.perSample);
-        uint32_t j = (uint32_t)(w % f.perSample);
-        uint32_t x, y;
-        if (f.tilesX) {
-            uint32_t tile = j >> 5, lane = j & 31u;
-            x = (tile % f.tilesX) * 8u + (lane & 7u);
-            y = (tile / f.tilesX) * 4u + (lane >> 3);
-        } else {
-            x = j % f.width;
-            y = j / f.width;
+        uint32_t lo = 0, hi = ns;  // the last segment starting at or before i
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (seg[mid].extOffset <= i) lo = mid;
+            else hi = mid;
         }
-        uint32_t pixel = y * f.width + x;
+        const GenSeg sg = seg[lo];
+        const Frame& f = q.req[sg.slot];
+        const uint32_t e = eb + i;
+        const unsigned long long w = sg.workBase + (i - sg.extOffset);
+        const uint32_t perSample = f.perSample, width = f.width, tilesX = f.tilesX;
+        uint32_t sample = f.sampleOffset + (uint32_t)(w / perSample);
+        uint32_t j = (uint32_t)(w % perSample);
+        uint32_t x, y;
+        if (tilesX) {
+            uint32_t tile = j >> 5, lane = j & 31u;
+            x = (tile % tilesX) * 8u + (lane & 7u);
+            y = (tile / tilesX) * 4u + (lane >> 3);
+        } else {
+            x = j % width;
+            y = j / width;
+        }
+        uint32_t pixel = y * width + x;
         uint32_t seed = path_seed(pixel, sample, f.seed);
         uint32_t js = seed;
         float r1 = lcg_randf(js);
         float r2 = lcg_randf(js);
-        float nx = (2.0f * ((float)x + r1) / (float)f.width - 1.0f) * f.aspect;
+        float nx = (2.0f * ((float)x + r1) / (float)width - 1.0f) * f.aspect;
         float ny = 1.0f - 2.0f * ((float)y + r2) / (float)f.height;
         float3 fwd = f3(f.fwd[0], f.fwd[1], f.fwd[2]), rt = f3(f.right[0], f.right[1], f.right[2]),
                up = f3(f.up[0], f.up[1], f.up[2]), pos = f3(f.pos[0], f.pos[1], f.pos[2]);
-        float3 dir = normalize(add(add(fwd, mul(mul(rt, nx), f.tanHalf)), mul(mul(up, ny), f.tanHalf)));
+        const float tanHalf = f.tanHalf;
+        float3 dir = normalize(add(add(fwd, mul(mul(rt, nx), tanHalf)), mul(mul(up, ny), tanHalf)));
         float3 ro = pos, rd = dir;
-        if (f.lens > 0.0f && f.focal > 0.0f) {
+        const float lens = f.lens, focal = f.focal;
+        if (lens > 0.0f && focal > 0.0f) {
             float r3 = lcg_randf(js), r4 = lcg_randf(js);
             float th = 2.0f * 3.14159265f * r3;
-            float rad = sqrtf(r4) * f.lens;
+            float rad = sqrtf(r4) * lens;
             float sn, ct;
             sincosf(th, &sn, &ct);
             float3 off = f3(rt.x * rad * ct + up.x * rad * sn, rt.y * rad * ct + up.y * rad * sn,
                             rt.z * rad * ct + up.z * rad * sn);
-            float3 fp = f3(pos.x + dir.x * f.focal, pos.y + dir.y * f.focal, pos.z + dir.z * f.focal);
+            float3 fp = f3(pos.x + dir.x * focal, pos.y + dir.y * focal, pos.z + dir.z * focal);
             ro = f3(pos.x + off.x, pos.y + off.y, pos.z + off.z);
             rd = normalize(f3(fp.x - ro.x, fp.y - ro.y, fp.z - ro.z));
         }
@@ -124,13 +178,11 @@ __global__ void __launch_bounds__(kShadeBlock) k_generate(Queues q, Frame f) {
         o.ray_d[e] = make_float4(rd.x, rd.y, rd.z, 1e20f);
         o.thr[e] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
         o.rad[e] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(pixel));
-        o.st[e] = make_uint4(seed, 0u, 0u, kFlagFirstHit | kFlagPrevDelta);
+        o.st[e] = make_uint4(seed, 0u, 0u, kFlagFirstHit | kFlagPrevDelta | (sg.slot << kSlotShift));
     }
 }
 
-void launch_generate(const Queues& q, const Frame& f, int grid, cudaStream_t st) {
-    k_generate<<<grid, kShadeBlock, 0, st>>>(q, f);
-}
+void launch_generate(const Queues& q, int grid, cudaStream_t st) { k_generate<<<grid, kShadeBlock, 0, st>>>(q); }
 
 // ---------------------------------------------------------------------------
 // Closest-hit attributes (trace.cu:167-264): projected barycentrics, geometric and
@@ -293,9 +345,8 @@ struct ShadowOut {
 // it ended (accumulated or dropped).
 template <uint32_t kBucket>
 __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uint32_t i, const Frame& f, PathRegs& r,
-                                         ShadowOut& so) {
-    float4 o4 = in.ray_o[i], d4 = in.ray_d[i], h4 = in.hit[i], t4 = in.thr[i], r4 = in.rad[i];
-    uint4 st = in.st[i];
+                                         ShadowOut& so, float4 o4, float4 d4, float4 h4, float4 t4, float4 r4,
+                                         uint4 st) {
     r.o = f3(o4.x, o4.y, o4.z);
     r.d = f3(d4.x, d4.y, d4.z);
     r.thr = f3(t4.x, t4.y, t4.z);
@@ -466,8 +517,11 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uin
 #ifndef WRK_SHADE_MIN_BLOCKS
 #define WRK_SHADE_MIN_BLOCKS 4
 #endif
-template <uint32_t kBucket>
-__global__ void __launch_bounds__(kShadeBlock, WRK_SHADE_MIN_BLOCKS) k_shade(DevScene s, Queues q, Frame f) {
+// Shades one bucket.  A path's request (camera, settings, sums) comes from the
+// slot in its state word; with kMulti its scene too, otherwise every path is in
+// scene s0.  Paths that end are counted for their request.
+template <uint32_t kBucket, bool kMulti, int kBlock>
+__global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k_shade(DevScene s0, Queues q) {
     Counters* c = q.ctr;
     const uint32_t cur = c->cur, nxt = cur ^ 1u;
     const uint32_t n = min(c->bucket[kBucket].v, q.capacity);
@@ -479,7 +533,20 @@ __global__ void __launch_bounds__(kShadeBlock, WRK_SHADE_MIN_BLOCKS) k_shade(Dev
         constexpr uint32_t kCode = kBucket == kBucketLambertResume ? kBucketLambert : kBucket;
         PathRegs r;
         ShadowOut so;
-        int out = i < n ? shade_one<kCode>(s, in, i, f, r, so) : kOutNone;
+        int out = kOutNone;
+        uint32_t slot = 0;
+        if (i < n) {
+            float4 o4 = in.ray_o[i], d4 = in.ray_d[i], h4 = in.hit[i], t4 = in.thr[i], r4 = in.rad[i];
+            uint4 st = in.st[i];
+            slot = slot_of(st.w);
+            const Frame& f = q.req[slot];
+            if constexpr (kMulti) {
+                out = shade_one<kCode>(q.scenes[f.scene], in, i, f, r, so, o4, d4, h4, t4, r4, st);
+            } else {
+                out = shade_one<kCode>(s0, in, i, f, r, so, o4, d4, h4, t4, r4, st);
+            }
+        }
+        count_ended(q.ctl, out == kOutDone, slot);
         uint32_t pe = append_pos(&c->ext[nxt].v, out == kOutExt, q.capacity, &c->error);
         uint32_t ps = append_pos(&c->shd[nxt].v, out == kOutShadow, q.capacity, &c->error);
         if (pe != kInvalidSlot) {
@@ -502,13 +569,27 @@ __global__ void __launch_bounds__(kShadeBlock, WRK_SHADE_MIN_BLOCKS) k_shade(Dev
     }
 }
 
-void launch_shade_bucket(uint32_t b, const DevScene& s, const Queues& q, const Frame& f, int grid, cudaStream_t st) {
+template <bool kMulti, int kBlock>
+static void launch_shade_t(uint32_t b, const DevScene& s, const Queues& q, int grid, cudaStream_t st) {
     switch (b) {
-        case kBucketLambert: k_shade<kBucketLambert><<<grid, kShadeBlock, 0, st>>>(s, q, f); break;
-        case kBucketDielectric: k_shade<kBucketDielectric><<<grid, kShadeBlock, 0, st>>>(s, q, f); break;
-        case kBucketGGX: k_shade<kBucketGGX><<<grid, kShadeBlock, 0, st>>>(s, q, f); break;
-        case kBucketLambertResume: k_shade<kBucketLambertResume><<<grid, kShadeBlock, 0, st>>>(s, q, f); break;
-        default: k_shade<kBucketOther><<<grid, kShadeBlock, 0, st>>>(s, q, f); break;
+        case kBucketLambert: k_shade<kBucketLambert, kMulti, kBlock><<<grid, kBlock, 0, st>>>(s, q); break;
+        case kBucketDielectric: k_shade<kBucketDielectric, kMulti, kBlock><<<grid, kBlock, 0, st>>>(s, q); break;
+        case kBucketGGX: k_shade<kBucketGGX, kMulti, kBlock><<<grid, kBlock, 0, st>>>(s, q); break;
+        case kBucketLambertResume:
+            k_shade<kBucketLambertResume, kMulti, kBlock><<<grid, kBlock, 0, st>>>(s, q);
+            break;
+        default: k_shade<kBucketOther, kMulti, kBlock><<<grid, kBlock, 0, st>>>(s, q); break;
+    }
+}
+
+void launch_shade_bucket(uint32_t b, const DevScene& s, const Queues& q, bool multi, int grid, int block,
+                         cudaStream_t st) {
+    if (block == 128) {
+        if (multi) launch_shade_t<true, 128>(b, s, q, grid * 2, st);
+        else launch_shade_t<false, 128>(b, s, q, grid * 2, st);
+    } else {
+        if (multi) launch_shade_t<true, 256>(b, s, q, grid, st);
+        else launch_shade_t<false, 256>(b, s, q, grid, st);
     }
 }
 

@@ -108,6 +108,13 @@ __device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, 
     }
 }
 
+// The four scene fields traversal needs (a DevScene has them too).
+struct TraceGeom {
+    const uint4* nodes;
+    const float4* tris;
+    uint32_t numNodes, numTris;
+};
+
 // Per-lane traversal state, kept in registers across the persistent loop's rounds.
 struct Trav {
     Ray r;
@@ -144,8 +151,8 @@ __device__ __forceinline__ void trav_init(Trav& t, const Ray& r) {
 // (pushing the group's remainder), test the triangles that node exposes, and pop
 // when the group is used up.  Returns true when the ray is finished.  Closest hit
 // keeps ties in t with the lower primitive index; any hit stops at the first hit.
-template <bool kAnyHit>
-__device__ __forceinline__ bool trav_step(const DevScene& s, Trav& t, uint2* sstack, uint2* lstack,
+template <bool kAnyHit, class Geom>
+__device__ __forceinline__ bool trav_step(const Geom& s, Trav& t, uint2* sstack, uint2* lstack,
                                           uint32_t* errFlag) {
     const int tid = threadIdx.x;
     if (++t.visits > kMaxVisits) {  // a malformed tree must not spin forever
@@ -318,9 +325,26 @@ __device__ __forceinline__ PathQ pick_bucket(const Queues& q, uint32_t b) {
 #endif
 constexpr int kRefillAt = WRK_REFILL_AT;
 
-template <bool kAnyHit>
-__global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_persistent(DevScene s, Queues q,
-                                                                                      Frame f) {
+// Adds a miss's environment term and accumulates the path into its request's sums
+// (__miss__trace + the raygen miss branch, trace.cu:143-148).
+__device__ __forceinline__ void miss_accumulate(const float env[3], const Frame& f, float4 th, float4 rd) {
+    float3 L = make_float3(rd.x + th.x * env[0], rd.y + th.y * env[1], rd.z + th.z * env[2]);
+    L = clamp_fireflies(L, f.fireflyClamp);
+    atomicAdd(f.accum + __float_as_uint(rd.w), make_float4(L.x, L.y, L.z, 0.0f));
+}
+
+__device__ __forceinline__ void count_ended_t(SlotCtl* ctl, bool ended, uint32_t slot) {
+    const uint32_t m = __ballot_sync(0xffffffffu, ended);
+    if (!m) return;
+    const uint32_t peers = __match_any_sync(0xffffffffu, ended ? slot : 0xffffffffu) & m;
+    if (ended && (uint32_t)(__ffs(peers) - 1) == (threadIdx.x & 31u))
+        atomicAdd(&ctl[slot].finished, (unsigned long long)__popc(peers));
+}
+
+// kMulti: the batch's requests may use different scenes; a lane loads the
+// geometry of its ray's scene when it fetches the ray.  Otherwise scene s0.
+template <bool kAnyHit, bool kMulti>
+__global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_persistent(DevScene s0, Queues q) {
     __shared__ uint2 sstack[kStackSmem * kTraceBlock];
     uint2 lstack[kStackLocal];
     Counters* c = q.ctr;
@@ -330,6 +354,8 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
     uint32_t* fetch = kAnyHit ? &c->fetchShadow.v : &c->fetchExtension.v;
     const uint32_t lane = threadIdx.x & 31u;
     Trav t;
+    TraceGeom geo{s0.nodes, s0.tris, s0.numNodes, s0.numTris};
+    uint32_t sceneIdx = 0;
     uint32_t idx = 0;
     bool active = false, exhausted = false;
     while (true) {
@@ -343,6 +369,11 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
                 if (idx < n) {
                     float4 o = kAnyHit ? in.sh_o[idx] : in.ray_o[idx];
                     float4 d = kAnyHit ? in.sh_d[idx] : in.ray_d[idx];
+                    if constexpr (kMulti) {
+                        sceneIdx = q.req[slot_of(in.st[idx].w)].scene;
+                        const DevScene& sc = q.scenes[sceneIdx];
+                        geo = TraceGeom{sc.nodes, sc.tris, sc.numNodes, sc.numTris};
+                    }
                     trav_init(t, Ray{o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w});
                     active = true;
                 } else {
@@ -355,7 +386,7 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
         const int refillAt = __any_sync(0xffffffffu, exhausted) ? 1 : kRefillAt;
         bool fin = false;
         do {
-            if (active && !fin) fin = trav_step<kAnyHit>(s, t, sstack, lstack, &c->error);
+            if (active && !fin) fin = trav_step<kAnyHit>(geo, t, sstack, lstack, &c->error);
         } while (__popc(__ballot_sync(0xffffffffu, active && !fin)) >= refillAt);
         const bool done = active && fin;
         if (kAnyHit) {
@@ -379,18 +410,24 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
         } else {
             uint32_t bucket = kNumBuckets;
             float4 th = make_float4(0, 0, 0, 0), rd = make_float4(0, 0, 0, 0);
+            uint4 st = make_uint4(0, 0, 0, 0);
+            bool missed = false;
             if (done) {
                 th = in.thr[idx];
                 rd = in.rad[idx];
-                if (t.pBest != kNoHit) {
-                    bucket = t.mBest < s.numMats ? bucket_of(s.mats[t.mBest].type) : kBucketOther;
+                st = in.st[idx];
+                const Frame& f = q.req[slot_of(st.w)];
+                if constexpr (kMulti) {
+                    const DevScene& sc = q.scenes[sceneIdx];
+                    if (t.pBest != kNoHit) bucket = t.mBest < sc.numMats ? bucket_of(sc.mats[t.mBest].type) : kBucketOther;
+                    else miss_accumulate(sc.env, f, th, rd);
                 } else {
-                    // __miss__trace + the raygen miss branch (trace.cu:143-148): T*env, accumulate, terminate
-                    float3 L = make_float3(rd.x + th.x * s.env[0], rd.y + th.y * s.env[1], rd.z + th.z * s.env[2]);
-                    L = clamp_fireflies(L, f.fireflyClamp);
-                    atomicAdd(f.accum + __float_as_uint(rd.w), make_float4(L.x, L.y, L.z, 0.0f));
+                    if (t.pBest != kNoHit) bucket = t.mBest < s0.numMats ? bucket_of(s0.mats[t.mBest].type) : kBucketOther;
+                    else miss_accumulate(s0.env, f, th, rd);
                 }
+                missed = t.pBest == kNoHit;
             }
+            count_ended_t(q.ctl, missed, slot_of(st.w));
             uint32_t pos = kInvalidSlot;
 #pragma unroll
             for (uint32_t b = 0; b < kBucketLambertResume; ++b) {
@@ -404,18 +441,20 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
                 o.hit[pos] = make_float4(t.tBest, __uint_as_float(t.pBest), __uint_as_float(t.mBest), 0.0f);
                 o.thr[pos] = th;
                 o.rad[pos] = rd;
-                o.st[pos] = in.st[idx];
+                o.st[pos] = st;
             }
         }
         if (done) active = false;
     }
 }
 
-void launch_trace_extension(const DevScene& s, const Queues& q, const Frame& f, int grid, cudaStream_t st) {
-    k_trace_persistent<false><<<grid, kTraceBlock, 0, st>>>(s, q, f);
+void launch_trace_extension(const DevScene& s, const Queues& q, bool multi, int grid, cudaStream_t st) {
+    if (multi) k_trace_persistent<false, true><<<grid, kTraceBlock, 0, st>>>(s, q);
+    else k_trace_persistent<false, false><<<grid, kTraceBlock, 0, st>>>(s, q);
 }
-void launch_trace_shadow(const DevScene& s, const Queues& q, const Frame& f, int grid, cudaStream_t st) {
-    k_trace_persistent<true><<<grid, kTraceBlock, 0, st>>>(s, q, f);
+void launch_trace_shadow(const DevScene& s, const Queues& q, bool multi, int grid, cudaStream_t st) {
+    if (multi) k_trace_persistent<true, true><<<grid, kTraceBlock, 0, st>>>(s, q);
+    else k_trace_persistent<true, false><<<grid, kTraceBlock, 0, st>>>(s, q);
 }
 
 }  // namespace wrk

@@ -39,8 +39,16 @@ enum : uint32_t {
     kBucketLambertResume = 4,
     kNumBuckets = 5
 };
-// st.w flags
+// st.w: flags in bits 0-7, the path's request slot in bits 8-15
 enum : uint32_t { kFlagFirstHit = 1u, kFlagPrevDelta = 2u, kFlagNeeDone = 4u };
+constexpr uint32_t kSlotShift = 8;
+__host__ __device__ inline uint32_t slot_of(uint32_t stw) { return (stw >> kSlotShift) & 0xffu; }
+
+// Requests in flight in one wavefront (each with its own camera, settings,
+// accumulation buffers and scene) and scenes one engine can address.
+constexpr uint32_t kMaxSlots = 64;
+constexpr uint32_t kMaxScenes = 128;
+enum : uint32_t { kSlotFree = 0, kSlotActive = 1, kSlotDone = 2 };
 
 constexpr uint32_t kInvalidSlot = 0xffffffffu;
 constexpr uint32_t kNoHit = 0xffffffffu;
@@ -107,17 +115,53 @@ struct Counters {
     uint32_t cur;          // which ext/shd buffer the current iteration consumes
     uint32_t genCount;     // paths generated this iteration
     uint32_t genExtBase;   // extension-queue index where the generated paths go
-    uint32_t pad0;
+    uint32_t numSeg;       // generation segments this iteration
     uint32_t iteration;
     uint32_t error;
-    uint32_t pad[2];
-    unsigned long long nextWork;
-    unsigned long long totalWork;
-    unsigned long long genWorkBase;
+    uint32_t activeSlots;  // slots still active after this iteration's completion check
+    uint32_t pad;
     unsigned long long extRays;
     unsigned long long shdRays;
     unsigned long long paths;
     unsigned long long bucketTotal[kNumBuckets];
+};
+
+// One request of a batch as the kernels see it: camera basis, render settings,
+// its scene and its per-pixel sums.  Lives in device memory (Queues::req).
+struct Frame {
+    float pos[3], fwd[3], right[3], up[3];
+    float tanHalf, aspect, focal, lens;
+    uint32_t width, height;
+    uint32_t tilesX, perSample;  // 8x4 pixel tiles across the image (0 = row order); work items per sample
+    uint32_t spp, useNEE, maxBounces, seed, maxIter, sampleOffset;
+    float rrStart, fireflyClamp;
+    uint32_t scene;  // index into Queues::scenes
+    uint32_t pad;
+    float4* accum;   // radiance sum per pixel
+    float4* albedo;  // first-hit albedo sum per pixel
+    float4* normal;  // first-hit normal sum per pixel
+    uint32_t* err;   // device error flags (Counters::error)
+};
+
+// Progress of a request slot.  The host arms it (workTotal, state = active); the
+// control kernel hands out its work items, kernels count the paths that ended,
+// and the control kernel marks it done (with a device timestamp) once every work
+// item was generated and every path of it ended.
+struct SlotCtl {
+    unsigned long long workTotal;  // pixels x spp
+    unsigned long long workNext;   // work items handed out
+    unsigned long long finished;   // paths ended (accumulated or dropped)
+    unsigned long long doneNs;     // %globaltimer when marked done
+    uint32_t state;
+    uint32_t doneIter;
+    uint32_t pad[2];
+};
+
+// Work items of one request generated in this iteration: extension-queue entries
+// [genExtBase + extOffset, + count) take work items [workBase, + count).
+struct GenSeg {
+    unsigned long long workBase;
+    uint32_t slot, count, extOffset, pad;
 };
 
 struct Queues {
@@ -126,27 +170,22 @@ struct Queues {
     PathQ bucket[kNumBuckets];
     Counters* ctr;
     uint32_t capacity;
-};
-
-struct Frame {
-    float pos[3], fwd[3], right[3], up[3];
-    float tanHalf, aspect, focal, lens;
-    uint32_t width, height;
-    uint32_t tilesX, perSample;  // 8x4 pixel tiles across the image (0 = row order); work items per sample
-    uint32_t spp, useNEE, maxBounces, seed, maxIter, sampleOffset;
-    float rrStart, fireflyClamp;
-    float4* accum;   // radiance sum per pixel
-    float4* albedo;  // first-hit albedo sum per pixel
-    float4* normal;  // first-hit normal sum per pixel
-    uint32_t* err;   // device error flags (Counters::error)
+    uint32_t pad;
+    const Frame* req;          // [kMaxSlots] request records
+    SlotCtl* ctl;              // [kMaxSlots]
+    const DevScene* scenes;    // [kMaxScenes]
+    const uint32_t* genOrder;  // genOrder[0] = n, then n slots in admission (FIFO) order
+    GenSeg* seg;               // [kMaxSlots] this iteration's generation segments
 };
 
 // ---- host-callable launchers (defined in the .cu files) ----
+// `multi`: requests of the batch may use different scenes (each path looks its
+// scene up through its request); otherwise every request uses scene `s`.
 void launch_control(const Queues& q, cudaStream_t st);
-void launch_generate(const Queues& q, const Frame& f, int grid, cudaStream_t st);
-void launch_trace_extension(const DevScene& s, const Queues& q, const Frame& f, int grid, cudaStream_t st);
-void launch_trace_shadow(const DevScene& s, const Queues& q, const Frame& f, int grid, cudaStream_t st);
-void launch_shade_bucket(uint32_t bucket, const DevScene& s, const Queues& q, const Frame& f, int grid,
+void launch_generate(const Queues& q, int grid, cudaStream_t st);
+void launch_trace_extension(const DevScene& s, const Queues& q, bool multi, int grid, cudaStream_t st);
+void launch_trace_shadow(const DevScene& s, const Queues& q, bool multi, int grid, cudaStream_t st);
+void launch_shade_bucket(uint32_t bucket, const DevScene& s, const Queues& q, bool multi, int grid, int block,
                          cudaStream_t st);
 void launch_resolve(const Frame& f, uint32_t rawGuides, float* rgb, float* albedo, float* normal, cudaStream_t st);
 

@@ -63,6 +63,33 @@ class BvhInfoC(C.Structure):
                 ("depth", C.c_uint32), ("numEmissive", C.c_uint32), ("buildMs", C.c_float), ("sahCost", C.c_float)]
 
 
+class ServerConfigC(C.Structure):
+    _fields_ = [("capacity", C.c_uint32), ("maxRequests", C.c_uint32), ("poolBytes", C.c_uint64),
+                ("chunk", C.c_uint32), ("shadeBlock", C.c_uint32)]
+
+
+class ServerStatusC(C.Structure):
+    _fields_ = [("queued", C.c_uint32), ("running", C.c_uint32), ("ready", C.c_uint32), ("iterations", C.c_uint64),
+                ("lastChunkMs", C.c_float), ("poolFreeBytes", C.c_uint64)]
+
+
+class RequestInfoC(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("denoised", C.c_uint32),
+                ("submitMs", C.c_double), ("admitMs", C.c_double), ("readyMs", C.c_double),
+                ("iterations", C.c_uint32)]
+
+
+class TuneTrialC(C.Structure):
+    _fields_ = [("capacity", C.c_uint32), ("chunk", C.c_uint32), ("shadeBlock", C.c_uint32), ("ms", C.c_float)]
+
+
+class TuneResultC(C.Structure):
+    _fields_ = [("capacity", C.c_uint32), ("chunk", C.c_uint32), ("shadeBlock", C.c_uint32), ("bestMs", C.c_float),
+                ("numTrials", C.c_uint32), ("trials", TuneTrialC * 32)]
+
+
+WRK_FLAG_DENOISE = 4
+
 # Every entry point include/wrk.h declares, with its ctypes signature.
 _VP, _U32, _U64, _I, _F = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_float
 SIGNATURES = {
@@ -101,6 +128,17 @@ SIGNATURES = {
     "wrk_texture_batch": ([_VP, _U32, _VP, _U32, _VP], _I),
     "wrk_camera_rays": ([C.POINTER(CameraC), _U32, _U32, _VP, _VP, _U32, _U32, _VP], _I),
     "wrk_tonemap_aces": ([_VP, _U32, _VP], _I),
+    "wrk_renderer_set_launch": ([_VP, _U32, _U32], _I),
+    "wrk_server_create": ([_I, _VP, C.POINTER(_VP)], _I),
+    "wrk_server_destroy": ([_VP], _I),
+    "wrk_server_set_denoiser": ([_VP, _VP], _I),
+    "wrk_server_submit": ([_VP, _VP, C.POINTER(CameraC), C.POINTER(RenderParamsC), C.POINTER(_U64)], _I),
+    "wrk_server_step": ([_VP, _VP], _I),
+    "wrk_server_poll": ([_VP, _U64, C.POINTER(C.c_int)], _I),
+    "wrk_server_wait": ([_VP, _U64], _I),
+    "wrk_server_result": ([_VP, _U64, _VP, _VP, _VP, _VP], _I),
+    "wrk_server_result_device": ([_VP, _U64, _VP, _VP, _VP, _VP], _I),
+    "wrk_autotune": ([_I, _VP, C.POINTER(CameraC), C.POINTER(RenderParamsC), _VP], _I),
     "wrk_conv3x3_forward": ([_VP, _U32, _U32, _U32, _U32, _VP, _VP, _U32, _U32, _VP], _I),
     "wrk_conv3x3_wgrad": ([_VP, _VP, _U32, _U32, _U32, _U32, _U32, _VP], _I),
     "wrk_denoiser_create": ([_I, _U32, C.POINTER(_VP)], _I),
@@ -364,6 +402,9 @@ class Renderer:
             _lib.wrk_renderer_destroy(h)
             self.handle = None
 
+    def set_launch(self, chunk: int = 8, shade_block: int = 256) -> None:
+        _check(lib().wrk_renderer_set_launch(self.handle, chunk, shade_block))
+
     def render(self, scene: Scene, camera=None, settings=None, spp=None, guides=True, raw_guides=False,
                max_iterations=8, seed=None, sample_offset=0, stage_timing=False) -> RenderResult:
         """Synchronous render into host buffers (rgb = sum/spp, as libWR returns it)."""
@@ -553,3 +594,86 @@ class Denoiser:
         self.infer_device(dr, da, dn, B, H, W, do)
         out = do.numpy()
         return out[0] if squeeze else out
+
+
+# ---- serving loop and autotuner ----
+def _struct_dict(st) -> dict:
+    return {k: getattr(st, k) for k, _ in st._fields_}
+
+
+class Server:
+    """Continuous-batching render server (wrk_server_*): requests of any size, spp,
+    camera and scene share one set of wavefront queues on the device."""
+
+    def __init__(self, device: int = 0, capacity: int = 0, max_requests: int = 0, pool_bytes: int = 0,
+                 chunk: int = 0, shade_block: int = 0):
+        self.device = device
+        cfg = ServerConfigC(capacity, max_requests, pool_bytes, chunk, shade_block)
+        h = C.c_void_p()
+        _check(lib().wrk_server_create(device, C.byref(cfg), C.byref(h)))
+        self.handle = h.value
+        self._shapes = {}
+        self._denoiser = None
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and _lib is not None:
+            _lib.wrk_server_destroy(h)
+            self.handle = None
+
+    def set_denoiser(self, dn: "Denoiser") -> None:
+        self._denoiser = dn
+        _check(lib().wrk_server_set_denoiser(self.handle, dn.handle))
+
+    def submit(self, scene: Scene, camera=None, settings=None, spp=None, seed=None, sample_offset=0,
+               max_iterations=8, denoise=False) -> int:
+        cam = camera_struct(camera or scene._data.camera)
+        st = settings or scene._data.settings
+        p = params_struct(st, spp=spp, max_iterations=max_iterations, seed=seed, sample_offset=sample_offset)
+        if denoise:
+            p.flags |= WRK_FLAG_DENOISE
+        t = C.c_uint64()
+        _check(lib().wrk_server_submit(self.handle, scene.handle, C.byref(cam), C.byref(p), C.byref(t)))
+        self._shapes[t.value] = (st.height, st.width)
+        return t.value
+
+    def step(self) -> dict:
+        s = ServerStatusC()
+        _check(lib().wrk_server_step(self.handle, C.byref(s)))
+        return _struct_dict(s)
+
+    def ready(self, ticket: int) -> bool:
+        r = C.c_int()
+        _check(lib().wrk_server_poll(self.handle, ticket, C.byref(r)))
+        return bool(r.value)
+
+    def wait(self, ticket: int) -> None:
+        _check(lib().wrk_server_wait(self.handle, ticket))
+
+    def result(self, ticket: int, guides: bool = True):
+        """(rgb, albedo, normal, info) of a ready request; releases it."""
+        h, w = self._shapes.pop(ticket)
+        rgb = np.zeros((h, w, 3), np.float32)
+        alb = np.zeros((h, w, 3), np.float32) if guides else None
+        nrm = np.zeros((h, w, 3), np.float32) if guides else None
+        info = RequestInfoC()
+        _check(lib().wrk_server_result(self.handle, ticket, rgb.ctypes.data, None if alb is None else alb.ctypes.data,
+                                       None if nrm is None else nrm.ctypes.data, C.byref(info)))
+        return rgb, alb, nrm, _struct_dict(info)
+
+    def result_device(self, ticket: int, d_rgb_ptr: int, d_albedo_ptr=None, d_normal_ptr=None) -> dict:
+        self._shapes.pop(ticket, None)
+        info = RequestInfoC()
+        _check(lib().wrk_server_result_device(self.handle, ticket, d_rgb_ptr, d_albedo_ptr, d_normal_ptr,
+                                              C.byref(info)))
+        return _struct_dict(info)
+
+
+def autotune(scene: Scene, camera=None, settings=None, spp=None, device: int = 0) -> dict:
+    cam = camera_struct(camera or scene._data.camera)
+    st = settings or scene._data.settings
+    p = params_struct(st, spp=spp)
+    r = TuneResultC()
+    _check(lib().wrk_autotune(device, scene.handle, C.byref(cam), C.byref(p), C.byref(r)))
+    return {"capacity": r.capacity, "chunk": r.chunk, "shadeBlock": r.shadeBlock, "bestMs": r.bestMs,
+            "trials": [_struct_dict(r.trials[i]) for i in range(r.numTrials)]}
