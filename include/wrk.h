@@ -211,7 +211,9 @@ int wrk_server_submit(wrk_server* s, wrk_scene* scene, const wrk_camera* cam, co
 /* Admits, runs one chunk for every request in flight, retires finished ones. */
 int wrk_server_step(wrk_server* s, wrk_server_status* status);
 int wrk_server_poll(wrk_server* s, uint64_t ticket, int* ready);
-/* Steps until the request is ready. */
+/* Steps until the request is ready.  A ready request keeps its pool region until
+ * its result is taken; when ready results fill the pool (or the slots) so that the
+ * awaited request can never be admitted, this returns WRK_ERR_STATE. */
 int wrk_server_wait(wrk_server* s, uint64_t ticket);
 /* Copies a ready request's images (width*height*3 floats each; rgb is the denoised
  * image when the request asked for it; albedo / normal may be NULL) to host memory

@@ -386,7 +386,13 @@ int wrk_server_wait(wrk_server* sv, uint64_t ticket) {
         int rc = wrk_server_poll(sv, ticket, &ready);
         if (rc) return rc;
         if (ready) return WRK_OK;
-        if ((rc = wrk_server_step(sv, nullptr))) return rc;
+        wrk_server_status st{};
+        if ((rc = wrk_server_step(sv, &st))) return rc;
+        // nothing in flight and the request still queued: the pool or the slots
+        // are held by ready results nobody has taken
+        if (st.running == 0 && sv->reqs[ticket].state == kQueued)
+            return sfail(WRK_ERR_STATE, "request %llu cannot be admitted: take the ready results first",
+                         (unsigned long long)ticket);
     }
     return sfail(WRK_ERR_DEVICE, "request %llu did not finish", (unsigned long long)ticket);
 }

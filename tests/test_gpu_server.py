@@ -69,18 +69,40 @@ def test_continuous_admission_and_limits(gpu, world):
     second = srv.submit(cb, camera=_cam((0.4, 0.5, -1.3)), settings=_settings(64, 64, 4, base))
     extra = [srv.submit(cb, camera=_cam((0.5, 0.45, -1.5 - 0.1 * k)), settings=_settings(64, 64, 2, base))
              for k in range(3)]
+    # a ready request holds its pool region until its result is taken: take results
+    # as they come so the queued ones can be admitted
     max_running = 0
-    while not all(srv.ready(t) for t in [first, second] + extra):
+    results = {}
+    pending = [first, second] + extra
+    for _ in range(100000):
+        if not pending:
+            break
         st = srv.step()
         max_running = max(max_running, st["running"])
+        for t in [t for t in pending if srv.ready(t)]:
+            results[t] = srv.result(t)
+            pending.remove(t)
+    assert not pending, "requests did not finish"
     assert max_running <= 2
-    r1 = srv.result(first)[3]
-    r2 = srv.result(second)[3]
+    r1, r2 = results[first][3], results[second][3]
     assert r2["admitMs"] < r1["readyMs"], "second request was not admitted while the first was in flight"
     for k, t in enumerate(extra):
-        rgb, _, _, _ = srv.result(t)
         solo = _solo(gpu, cb, _cam((0.5, 0.45, -1.5 - 0.1 * k)), _settings(64, 64, 2, base))
-        assert _close(rgb, solo.rgb)
+        assert _close(results[t][0], solo.rgb)
+
+
+def test_wait_reports_a_request_that_cannot_be_admitted(gpu, world):
+    cb, _ = world
+    base = cb._data.settings
+    srv = gpu.Server(capacity=1 << 14, pool_bytes=32 * 32 * 96)  # room for one 32x32 request
+    a = srv.submit(cb, settings=_settings(32, 32, 2, base))
+    b = srv.submit(cb, settings=_settings(32, 32, 2, base))
+    srv.wait(a)  # ready, but its pool region stays held until the result is taken
+    with pytest.raises(gpu.WrkError):
+        srv.wait(b)
+    srv.result(a)
+    srv.wait(b)
+    assert srv.result(b)[3]["spp"] == 2
 
 
 def test_request_larger_than_pool_rejected(gpu, world):
