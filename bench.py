@@ -48,6 +48,14 @@ CONFIGS = {
 
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+FALLBACK_BF16_TFLOPS = 1590.0
+
+# Denoiser FLOPs per (padded) full-resolution pixel, forward: 2 * 9 * Cin * Cout per
+# output pixel of each 3x3 convolution, at 1/4^level of the pixels (head Cout padded to 16).
+UNET_LAYERS = [(16, 32, 0), (32, 32, 0), (32, 64, 1), (64, 64, 1), (64, 128, 2), (128, 128, 2), (128, 256, 3),
+               (256, 256, 3), (384, 128, 2), (128, 128, 2), (192, 64, 1), (64, 64, 1), (96, 32, 0), (32, 32, 0),
+               (32, 16, 0)]
+UNET_FLOP_PER_PX = sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in UNET_LAYERS)
 
 # Algorithmic HBM bytes per unit of work of each loop stage (per path, per ray):
 #   trace_extension: read the ray (origin|tmin, direction|tmax = 32 B) + write the
@@ -56,6 +64,12 @@ FALLBACK_HBM_GBS = 6650.0
 #                    and written, 4 B queue entry (rounded as 100 B / shadow ray)
 #   shade_*:         read direction 16 + hit 16 + path state 48, write state 48 +
 #                    next ray 32                                                = 160 B / path
+# Measured DRAM traffic of the extension-ray traversal kernel per ray: ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) summed over all 64 launches of four
+# 512x512 16-spp renders of the same scene, divided by their 57,625,904 extension
+# rays (profiles/k_trace_persistent_dram_showcase_16spp.md); traffic per launch of
+# the full workload = this x rays per launch (traffic grows with the rays traced).
+TRACE_EXT_TRAFFIC_BYTES_PER_RAY = 148.4
 STAGE_BYTES = {"trace_extension": 48, "trace_shadow": 100, "shade_lambert": 160, "shade_dielectric": 160,
                "shade_ggx": 160, "shade_emissive": 160, "shade_lambert_resume": 160}
 
@@ -118,6 +132,63 @@ def hbm_peak():
         return float(d["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         return FALLBACK_HBM_GBS, "fallback"
+
+
+def bf16_peak():
+    try:
+        d = json.load(open(MEASURED_PEAKS))
+        return float(d["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_BF16_TFLOPS, "fallback"
+
+
+def served_legs(args, rend, local):
+    """Denoiser throughput, time-to-relMSE and the serving workload on the scale
+    scene (1920x1080, ~2.41M triangles), with the committed denoiser weights."""
+    import torch
+
+    from offlinerenderer_b200 import denoise_train, quality, serve_bench, wrk
+
+    dn = wrk.Denoiser(device=local)
+    meta = denoise_train.load_weights(dn)
+    sd = scenes.scale_test(1920, 1080, 64, seed=1)
+    scene = wrk.Scene.from_data(sd, device=local)
+    st, cam = sd.settings, sd.camera
+    out = {}
+    # denoiser inference at 1920x1080 (padded to 1920x1088 inside)
+    img = torch.rand((1080, 1920, 3), device=f"cuda:{local}")
+    o = torch.empty_like(img)
+    ptr = quality._Ptr
+    for _ in range(3):
+        dn.infer_device(ptr(img), ptr(img), ptr(img), 1, 1080, 1920, ptr(o))
+    ms = []
+    for _ in range(10):
+        dn.infer_device(ptr(img), ptr(img), ptr(img), 1, 1080, 1920, ptr(o))
+        ms.append(dn.last_ms())
+    ms = statistics.median(ms)
+    flops = UNET_FLOP_PER_PX * 1088 * 1920
+    peak, kind = bf16_peak()
+    out["denoiser"] = {"workload": "U-Net 32/64/128/256, 15 3x3 convs, 1920x1080 (1920x1088 padded), bf16 in, f32 acc",
+                       "infer_ms": ms, "roofline": {"bound": "tensor", "achieved": flops / (ms / 1e3) / 1e12,
+                                                   "peak": peak, "unit": "TFLOP/s",
+                                                   "frac": flops / (ms / 1e3) / 1e12 / peak, "peak_source": kind,
+                                                   "flop_per_launch": flops},
+                       "weights": {k: meta[k] for k in ("scenes", "target_spp", "steps", "final_loss") if k in meta}}
+    # time to the plain 256-spp relMSE against an FP64-accumulated reference
+    rs = {}
+    ref = quality.reference(rend, scene, cam, st, total_spp=args.ref_spp, chunk=256, stats=rs)
+    ttr = quality.time_to_relmse(rend, dn, scene, cam, st, ref)
+    ttr["reference_nonfinite_pixel_chunks_dropped"] = rs["dropped"]
+    ttr["workload"] = "scale_test 1920x1080 maxDepth8 (~2.41M tris), camera of the benchmark scene, seed 1"
+    ttr["reference"] = f"{args.ref_spp} spp, f32 sums per 256-spp chunk accumulated in f64"
+    out["time_to_relmse"] = ttr
+    # serving: Poisson arrivals, random orbit cameras, mixed sizes and spp, denoised
+    srv = wrk.Server(device=local)
+    srv.set_denoiser(dn)
+    out["serving"] = serve_bench.run(srv, scene, n_requests=args.serve_requests, rate=50.0, device=local)
+    out["serving"]["scene"] = "scale_test (~2.41M tris), resident"
+    del srv
+    return out
 
 
 def cpu_reference_rate(sd, threads: int, target_s: float = 12.0):
@@ -196,6 +267,9 @@ def main():
     ap.add_argument("--config", default="showcase", choices=list(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=0, help="override the config's spp (smaller profiling cases)")
+    ap.add_argument("--no-served", action="store_true", help="skip the denoiser / time-to-relMSE / serving legs")
+    ap.add_argument("--serve-requests", type=int, default=400)
+    ap.add_argument("--ref-spp", type=int, default=4096)
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
@@ -301,6 +375,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_rate(sd, os.cpu_count() or 1)
+    served = {}
+    if rank == 0 and world == 1 and not args.no_served:
+        served = served_legs(args, rend, local)
 
     if rank == 0:
         out = {
@@ -326,7 +403,10 @@ def main():
             "e2e": {"value": e2e_val, "unit": "Msamples/s", "h2d_bytes_per_step": 76 + 44,
                     "d2h_bytes_per_step": npx * 3 * 4 * 3},
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                         "traffic": (TRACE_EXT_TRAFFIC_BYTES_PER_RAY * units[dominant] / launches
+                                     if dominant == "trace_extension" else None),
+                         "traffic_source": "ncu DRAM bytes per extension ray (16-spp capture) x rays per launch",
                          "peak_source": peak_kind, "avg_launch_ms": stage_ms[dominant] / launches,
                          "algorithmic_bytes_per_launch": dom_bytes / launches,
                          "units_per_launch": units[dominant] / launches},
@@ -336,6 +416,7 @@ def main():
             "clocks": clk,
             "cpu_baseline": cpu,
         }
+        out.update(served)
         print(json.dumps(out))
     del frame
     if dist is not None:

@@ -309,6 +309,9 @@ int wrk_denoiser_gradients(wrk_denoiser* d, const float* d_rgb, const float* d_a
 /* The same followed by one Adam step with learning rate lr. */
 int wrk_denoiser_train_step(wrk_denoiser* d, const float* d_rgb, const float* d_albedo, const float* d_normal,
                             const float* d_target, uint32_t B, uint32_t H, uint32_t W, float lr, float* loss);
+/* Device time (CUDA events on the denoiser's stream) of the last inference or
+ * training step. */
+int wrk_denoiser_last_ms(wrk_denoiser* d, float* ms);
 /* Denoises device images [B][H][W][3] f32 of any size (padded internally) into d_out. */
 int wrk_denoiser_infer(wrk_denoiser* d, const float* d_rgb, const float* d_albedo, const float* d_normal, uint32_t B,
                        uint32_t H, uint32_t W, float* d_out);

@@ -324,7 +324,12 @@ struct wrk_denoiser {
     conv::WgradPlan wplan[kLayers];
     CUtensorMap fin[kLayers], fw[kLayers], din[kLayers], dwmap[kLayers][2], wg[kLayers], wx[kLayers];
     uint32_t dsplit[kLayers];
+    // device time of the last inference / training step (events on `stream`)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float lastMs = 0.0f;
     ~wrk_denoiser() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -722,7 +727,8 @@ int wrk_denoiser_create(int device, uint32_t seed, wrk_denoiser** out) {
     wrk_denoiser* d = new wrk_denoiser();
     d->device = device;
     cudaDeviceGetAttribute(&d->numSMs, cudaDevAttrMultiProcessorCount, device);
-    if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&d->ev0) != cudaSuccess || cudaEventCreate(&d->ev1) != cudaSuccess) {
         delete d;
         return dfail(WRK_ERR_CUDA, "stream creation failed");
     }
@@ -784,6 +790,9 @@ int wrk_denoiser_gradients(wrk_denoiser* d, const float* rgb, const float* alb, 
 
 int wrk_denoiser_train_step(wrk_denoiser* d, const float* rgb, const float* alb, const float* nrm, const float* target,
                             uint32_t B, uint32_t H, uint32_t W, float lr, float* loss) {
+    if (!d) return dfail(WRK_ERR_INVALID, "null denoiser");
+    DCK(cudaSetDevice(d->device));
+    DCK(cudaEventRecord(d->ev0, d->stream));
     int rc = fwd_bwd(d, rgb, alb, nrm, target, B, H, W, loss);
     if (rc) return rc;
     d->step += 1;
@@ -793,7 +802,15 @@ int wrk_denoiser_train_step(wrk_denoiser* d, const float* rgb, const float* alb,
                                                         d->adamM.as<float>(), d->adamV.as<float>(), d->nparams, lr, b1,
                                                         b2, 1e-8f, c1, c2);
     if ((rc = relayout_all(d))) return rc;
+    DCK(cudaEventRecord(d->ev1, d->stream));
     DCK(cudaStreamSynchronize(d->stream));
+    cudaEventElapsedTime(&d->lastMs, d->ev0, d->ev1);
+    return WRK_OK;
+}
+
+int wrk_denoiser_last_ms(wrk_denoiser* d, float* ms) {
+    if (!d || !ms) return dfail(WRK_ERR_INVALID, "null argument");
+    *ms = d->lastMs;
     return WRK_OK;
 }
 
@@ -805,12 +822,16 @@ int wrk_denoiser_infer(wrk_denoiser* d, const float* rgb, const float* alb, cons
     int rc = set_shape(d, B, Hp, Wp);
     if (rc) return rc;
     DCK(cudaMemsetAsync(d->err.p, 0, 4, d->stream));
+    DCK(cudaEventRecord(d->ev0, d->stream));
     size_t P = (size_t)B * Hp * Wp;
     k_pack<<<grid_for(P), 256, 0, d->stream>>>(rgb, alb, nrm, B, H, W, Hp, Wp, d->x0.as<__nv_bfloat16>());
     if ((rc = forward(d))) return rc;
     k_unpack<<<grid_for((size_t)B * H * W), 256, 0, d->stream>>>(d->out.as<float>(), rgb, B, H, W, Hp, Wp, out);
     DCK(cudaGetLastError());
-    return check_err(d, "denoiser inference");
+    DCK(cudaEventRecord(d->ev1, d->stream));
+    rc = check_err(d, "denoiser inference");
+    if (!rc) cudaEventElapsedTime(&d->lastMs, d->ev0, d->ev1);
+    return rc;
 }
 
 }  // extern "C"

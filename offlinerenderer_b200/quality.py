@@ -22,15 +22,27 @@ class _Ptr:
 
 
 def relmse(x, ref) -> float:
+    """relMSE over the entries where the image is finite (non-finite entries are
+    counted by `nonfinite`; a path that produced NaN is not a quality figure)."""
     import torch
 
     if isinstance(x, torch.Tensor):
         x64 = x.double()
         r64 = ref.double()
-        return float(torch.mean((x64 - r64) ** 2 / (r64 * r64 + 1e-2)).item())
+        e = (x64 - r64) ** 2 / (r64 * r64 + 1e-2)
+        return float(e[torch.isfinite(e)].mean().item())
     x = np.asarray(x, np.float64)
     r = np.asarray(ref, np.float64)
-    return float(np.mean((x - r) ** 2 / (r * r + 1e-2)))
+    e = (x - r) ** 2 / (r * r + 1e-2)
+    return float(np.mean(e[np.isfinite(e)]))
+
+
+def nonfinite(x) -> int:
+    import torch
+
+    if isinstance(x, torch.Tensor):
+        return int((~torch.isfinite(x)).sum().item())
+    return int((~np.isfinite(np.asarray(x))).sum())
 
 
 def _settings(st, spp):
@@ -51,19 +63,28 @@ def render(renderer, scene, cam, st, spp, sample_offset, torch, device=0, guides
     return rgb, alb, nrm, s["gpuMs"]
 
 
-def reference(renderer, scene, cam, st, total_spp=4096, chunk=256, sample_offset=1 << 20, device=0):
+def reference(renderer, scene, cam, st, total_spp=4096, chunk=256, sample_offset=1 << 20, device=0, stats=None):
     """FP64-accumulated reference: chunks of `chunk` spp (f32 per-pixel sums inside a
-    chunk) summed in float64 over disjoint sample ranges."""
+    chunk) summed in float64 over disjoint sample ranges.  A chunk whose pixel sum
+    is not finite (a path produced NaN or inf) is left out of that pixel's average;
+    `stats["dropped"]` counts such pixel-chunks."""
     import torch
 
     acc = torch.zeros((st.height, st.width, 3), dtype=torch.float64, device=f"cuda:{device}")
+    cnt = torch.zeros_like(acc)
     n = 0
+    dropped = 0
     while n < total_spp:
         k = min(chunk, total_spp - n)
         rgb, _, _, _ = render(renderer, scene, cam, st, k, sample_offset + n, torch, device, guides=False)
-        acc += rgb.double() * k
+        ok = torch.isfinite(rgb)
+        dropped += int((~ok).sum().item())
+        acc += torch.where(ok, rgb.double() * k, torch.zeros_like(acc))
+        cnt += ok.double() * k
         n += k
-    return acc / total_spp
+    if stats is not None:
+        stats["dropped"] = dropped
+    return acc / cnt.clamp(min=1)
 
 
 def time_to_relmse(renderer, denoiser, scene, cam, st, ref, plain_spp=256, search=(1, 2, 4, 8, 16, 32, 64, 128),
@@ -89,6 +110,7 @@ def time_to_relmse(renderer, denoiser, scene, cam, st, ref, plain_spp=256, searc
     H, W = st.height, st.width
     (plain, _, _, _), plain_ms = timed(lambda: render(renderer, scene, cam, st, plain_spp, 0, torch, device, False))
     bar = relmse(plain, ref)
+    plain_nonfinite = nonfinite(plain)
     rows = []
     found = None
     for s in search:
@@ -99,11 +121,13 @@ def time_to_relmse(renderer, denoiser, scene, cam, st, ref, plain_spp=256, searc
             return rgb, out
 
         (noisy, den), ms = timed(run)
-        r = {"spp": s, "ms": ms, "relmse_noisy": relmse(noisy, ref), "relmse_denoised": relmse(den, ref)}
+        r = {"spp": s, "ms": ms, "relmse_noisy": relmse(noisy, ref), "relmse_denoised": relmse(den, ref),
+             "nonfinite_denoised": nonfinite(den)}
         rows.append(r)
         if found is None and r["relmse_denoised"] <= bar:
             found = r
             break
-    return {"plain_spp": plain_spp, "plain_ms": plain_ms, "plain_relmse": bar, "search": rows,
+    return {"plain_spp": plain_spp, "plain_ms": plain_ms, "plain_relmse": bar, "plain_nonfinite": plain_nonfinite,
+            "search": rows,
             "denoised_spp": found["spp"] if found else None, "denoised_ms": found["ms"] if found else None,
             "time_ratio": (found["ms"] / plain_ms) if found else None}

@@ -149,6 +149,7 @@ SIGNATURES = {
     "wrk_denoiser_gradients": ([_VP, _VP, _VP, _VP, _VP, _U32, _U32, _U32, _VP, C.POINTER(_F)], _I),
     "wrk_denoiser_train_step": ([_VP, _VP, _VP, _VP, _VP, _U32, _U32, _U32, _F, C.POINTER(_F)], _I),
     "wrk_denoiser_infer": ([_VP, _VP, _VP, _VP, _U32, _U32, _U32, _VP], _I),
+    "wrk_denoiser_last_ms": ([_VP, C.POINTER(_F)], _I),
 }
 
 _lib = None
@@ -576,6 +577,12 @@ class Denoiser:
         _check(lib().wrk_denoiser_train_step(self.handle, d_rgb.ptr, self._ptr(d_alb), self._ptr(d_nrm), d_target.ptr,
                                              B, H, W, lr, C.byref(loss)))
         return loss.value
+
+    def last_ms(self) -> float:
+        """Device time of the last inference / training step."""
+        ms = C.c_float()
+        _check(lib().wrk_denoiser_last_ms(self.handle, C.byref(ms)))
+        return ms.value
 
     def infer_device(self, d_rgb, d_alb, d_nrm, B, H, W, d_out) -> None:
         _check(lib().wrk_denoiser_infer(self.handle, d_rgb.ptr, self._ptr(d_alb), self._ptr(d_nrm), B, H, W,
