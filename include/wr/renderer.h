@@ -16,11 +16,17 @@ struct RendererConfig {
     float russianRouletteDepth = 3;
 };
 
+// libWR's OptiX AI denoiser settings.  Here `enabled` runs the learned U-Net
+// denoiser, which always uses the albedo and normal guides it was trained with
+// (useAlbedo / useNormal / hdrIntensity are accepted and not needed).
 struct DenoiserConfig {
     bool enabled = false;
     bool useAlbedo = false;
     bool useNormal = false;
     float hdrIntensity = 1.0f;
+    // --- additive extension ---
+    const char* weightsPath = nullptr;  // WRKUNET1 file; null = $WRK_DENOISER_WEIGHTS, else
+                                        // weights/unet_scale.wrkw next to libwrk.so
 };
 
 struct RenderParams {

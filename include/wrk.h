@@ -309,6 +309,9 @@ int wrk_denoiser_gradients(wrk_denoiser* d, const float* d_rgb, const float* d_a
 /* The same followed by one Adam step with learning rate lr. */
 int wrk_denoiser_train_step(wrk_denoiser* d, const float* d_rgb, const float* d_albedo, const float* d_normal,
                             const float* d_target, uint32_t B, uint32_t H, uint32_t W, float lr, float* loss);
+/* Loads weights written by offlinerenderer_b200.denoise_train ("WRKUNET1" file:
+ * count, metadata length, bf16 parameters, JSON metadata); resets the optimizer. */
+int wrk_denoiser_load(wrk_denoiser* d, const char* path);
 /* Device time (CUDA events on the denoiser's stream) of the last inference or
  * training step. */
 int wrk_denoiser_last_ms(wrk_denoiser* d, float* ms);

@@ -808,6 +808,28 @@ int wrk_denoiser_train_step(wrk_denoiser* d, const float* rgb, const float* alb,
     return WRK_OK;
 }
 
+// Weights file: "WRKUNET1", u64 count, u64 metadata bytes, count bf16 bit patterns
+// (the precision inference uses), then the metadata (JSON text).
+int wrk_denoiser_load(wrk_denoiser* d, const char* path) {
+    if (!d || !path) return dfail(WRK_ERR_INVALID, "null argument");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return dfail(WRK_ERR_INVALID, "cannot open denoiser weights %s", path);
+    char magic[8];
+    uint64_t count = 0, metaLen = 0;
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "WRKUNET1", 8) == 0 &&
+              std::fread(&count, 8, 1, f) == 1 && std::fread(&metaLen, 8, 1, f) == 1 && count == d->nparams;
+    std::vector<uint16_t> bits(ok ? count : 0);
+    ok = ok && std::fread(bits.data(), 2, count, f) == count;
+    std::fclose(f);
+    if (!ok) return dfail(WRK_ERR_INVALID, "%s is not a weights file for this network (%zu parameters)", path, d->nparams);
+    std::vector<float> h(count);
+    for (size_t i = 0; i < count; ++i) {
+        uint32_t u = (uint32_t)bits[i] << 16;
+        std::memcpy(&h[i], &u, 4);
+    }
+    return wrk_denoiser_set_params(d, h.data(), count);
+}
+
 int wrk_denoiser_last_ms(wrk_denoiser* d, float* ms) {
     if (!d || !ms) return dfail(WRK_ERR_INVALID, "null argument");
     *ms = d->lastMs;

@@ -10,7 +10,9 @@
 #include <zlib.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <dlfcn.h>
 #include <fstream>
 #include <iterator>
 #include <stdexcept>
@@ -358,10 +360,29 @@ struct RendererImpl {
     int device = 0;
     wrk_renderer* handle = nullptr;
     RenderStats stats;
+    // the learned denoiser (created on the first denoised render) and its device buffers
+    wrk_denoiser* denoiser = nullptr;
+    std::string weights;
+    void* dbuf = nullptr;
+    size_t dbufBytes = 0;
     ~RendererImpl() {
+        if (dbuf) wrk_free(dbuf);
+        if (denoiser) wrk_denoiser_destroy(denoiser);
         if (handle) wrk_renderer_destroy(handle);
     }
 };
+
+// Default weights: $WRK_DENOISER_WEIGHTS, else weights/unet_scale.wrkw beside this library.
+static std::string default_weights() {
+    if (const char* e = std::getenv("WRK_DENOISER_WEIGHTS")) return e;
+    Dl_info info{};
+    if (dladdr(reinterpret_cast<void*>(&wrk_version), &info) && info.dli_fname) {
+        std::string lib = info.dli_fname;
+        size_t slash = lib.find_last_of('/');
+        return (slash == std::string::npos ? std::string(".") : lib.substr(0, slash)) + "/weights/unet_scale.wrkw";
+    }
+    return "weights/unet_scale.wrkw";
+}
 
 Renderer::Renderer(const RendererConfig& config) : Renderer(config, 0) {}
 Renderer::Renderer(const RendererConfig& config, int deviceId) : m_impl(new RendererImpl()), m_config(config) {
@@ -378,8 +399,6 @@ const RenderStats& Renderer::lastStats() const { return m_impl->stats; }
 
 void Renderer::render(Scene* scene, const Camera& camera, Vec3* out, const RenderParams& p) {
     if (!scene || !out) throw std::runtime_error("render: null scene or output buffer");
-    if (p.denoiser.enabled)
-        throw std::runtime_error("render: the denoise stage is not available in this build (render without it)");
     scene->finalize();
     wrk_camera c{};
     c.position[0] = camera.position.x; c.position[1] = camera.position.y; c.position[2] = camera.position.z;
@@ -401,9 +420,44 @@ void Renderer::render(Scene* scene, const Camera& camera, Vec3* out, const Rende
     rp.maxIterations = p.maxIterations;
     rp.flags = p.rawGuides ? WRK_FLAG_RAW_GUIDES : 0u;
     wrk_render_stats st{};
-    check(wrk_render(m_impl->handle, scene->native(), &c, &rp, reinterpret_cast<float*>(out),
-                     reinterpret_cast<float*>(p.albedoOut), reinterpret_cast<float*>(p.normalOut), &st),
-          "wrk_render");
+    if (!p.denoiser.enabled) {
+        check(wrk_render(m_impl->handle, scene->native(), &c, &rp, reinterpret_cast<float*>(out),
+                         reinterpret_cast<float*>(p.albedoOut), reinterpret_cast<float*>(p.normalOut), &st),
+              "wrk_render");
+    } else {
+        // libWR denoises inside render (renderer.cpp:289-313, denoiser.cpp:17-195): render
+        // rgb + averaged guides into device memory, denoise, copy the result out.
+        const std::string path = p.denoiser.weightsPath ? p.denoiser.weightsPath : default_weights();
+        if (!m_impl->denoiser) check(wrk_denoiser_create(m_impl->device, 1, &m_impl->denoiser), "wrk_denoiser_create");
+        if (m_impl->weights != path) {
+            check(wrk_denoiser_load(m_impl->denoiser, path.c_str()), "wrk_denoiser_load");
+            m_impl->weights = path;
+        }
+        const size_t np = (size_t)p.width * p.height, bytes = np * 12 * sizeof(float);
+        if (m_impl->dbufBytes < bytes) {
+            if (m_impl->dbuf) wrk_free(m_impl->dbuf);
+            m_impl->dbuf = nullptr;
+            m_impl->dbufBytes = 0;
+            check(wrk_malloc(m_impl->device, bytes, &m_impl->dbuf), "wrk_malloc");
+            m_impl->dbufBytes = bytes;
+        }
+        float* d = static_cast<float*>(m_impl->dbuf);
+        wrk_render_params dp = rp;
+        dp.flags &= ~WRK_FLAG_RAW_GUIDES;  // the network takes guides averaged over spp
+        check(wrk_render_device(m_impl->handle, scene->native(), &c, &dp, d, d + 3 * np, d + 6 * np, &st),
+              "wrk_render_device");
+        check(wrk_denoiser_infer(m_impl->denoiser, d, d + 3 * np, d + 6 * np, 1, p.height, p.width, d + 9 * np),
+              "wrk_denoiser_infer");
+        check(wrk_memcpy_dtoh(out, d + 9 * np, np * 3 * sizeof(float)), "wrk_memcpy_dtoh");
+        const float g = p.rawGuides ? (float)p.spp : 1.0f;
+        Vec3* guides[2] = {p.albedoOut, p.normalOut};
+        for (int k = 0; k < 2; ++k) {
+            if (!guides[k]) continue;
+            check(wrk_memcpy_dtoh(guides[k], d + 3 * (k + 1) * np, np * 3 * sizeof(float)), "wrk_memcpy_dtoh");
+            if (g != 1.0f)
+                for (size_t i = 0; i < np; ++i) guides[k][i] = guides[k][i] * g;
+        }
+    }
     m_impl->stats.paths = st.paths;
     m_impl->stats.extensionRays = st.extensionRays;
     m_impl->stats.shadowRays = st.shadowRays;

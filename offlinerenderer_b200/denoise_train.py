@@ -27,7 +27,7 @@ import numpy as np
 from . import scenes, wrk
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_WEIGHTS = os.path.join(HERE, "weights", "unet_scale.npz")
+DEFAULT_WEIGHTS = os.path.join(HERE, "weights", "unet_scale.wrkw")
 INPUT_SPPS = (1, 2, 4, 8, 16, 32)
 
 
@@ -141,16 +141,35 @@ def train(data, steps, batch=16, crop=128, lr=1e-3, seed=1, device=0, log=print,
     return dn, losses, time.time() - t0
 
 
+def write_weights(path: str, params: np.ndarray, meta: dict) -> None:
+    """WRKUNET1 file: magic, u64 count, u64 metadata bytes, count bf16 bit patterns
+    (the precision inference uses), JSON metadata.  wrk_denoiser_load reads it."""
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    bits = wrk.to_bf16_bits(np.asarray(params, np.float32))
+    m = json.dumps(meta).encode()
+    with open(path, "wb") as f:
+        f.write(b"WRKUNET1")
+        f.write(np.asarray([bits.size, len(m)], np.uint64).tobytes())
+        f.write(bits.tobytes())
+        f.write(m)
+
+
+def read_meta(path: str) -> dict:
+    with open(path, "rb") as f:
+        if f.read(8) != b"WRKUNET1":
+            raise ValueError(f"{path} is not a WRKUNET1 weights file")
+        count, mlen = np.frombuffer(f.read(16), np.uint64)
+        f.seek(24 + 2 * int(count))
+        return json.loads(f.read(int(mlen)).decode())
+
+
 def save_weights(dn: "wrk.Denoiser", path: str, meta: dict) -> None:
-    """Weights as bf16 bit patterns (the precision inference uses) plus metadata."""
-    os.makedirs(os.path.dirname(path), exist_ok=True)
-    np.savez_compressed(path, params_bf16=wrk.to_bf16_bits(dn.get_params()), meta=json.dumps(meta))
+    write_weights(path, dn.get_params(), meta)
 
 
 def load_weights(dn: "wrk.Denoiser", path: str = DEFAULT_WEIGHTS) -> dict:
-    z = np.load(path)
-    dn.set_params(wrk.from_bf16_bits(z["params_bf16"]))
-    return json.loads(str(z["meta"]))
+    dn.load(path)
+    return read_meta(path)
 
 
 def main():

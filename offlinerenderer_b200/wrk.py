@@ -150,6 +150,7 @@ SIGNATURES = {
     "wrk_denoiser_train_step": ([_VP, _VP, _VP, _VP, _VP, _U32, _U32, _U32, _F, C.POINTER(_F)], _I),
     "wrk_denoiser_infer": ([_VP, _VP, _VP, _VP, _U32, _U32, _U32, _VP], _I),
     "wrk_denoiser_last_ms": ([_VP, C.POINTER(_F)], _I),
+    "wrk_denoiser_load": ([_VP, C.c_char_p], _I),
 }
 
 _lib = None
@@ -556,6 +557,10 @@ class Denoiser:
         out = np.zeros(self.num_params, np.float32)
         _check(lib().wrk_denoiser_get_params(self.handle, out.ctypes.data, self.num_params))
         return out
+
+    def load(self, path: str) -> None:
+        """Loads a WRKUNET1 weights file through the C ABI."""
+        _check(lib().wrk_denoiser_load(self.handle, os.fsencode(path)))
 
     def set_params(self, p: np.ndarray) -> None:
         p = np.ascontiguousarray(p, np.float32)

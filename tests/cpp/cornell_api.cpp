@@ -70,9 +70,14 @@ int main(int argc, char** argv) {
     } catch (const std::runtime_error&) {
         threw = true;
     }
+    // libWR's legacy call with the denoiser on (renderer.cpp:318-335)
+    std::vector<wr::Vec3> denoised(W * H);
+    renderer->render(scene, camera, denoised.data(), W, H, 8, true);
     FILE* f = std::fopen(argv[1], "wb");
     std::fwrite(image.data(), sizeof(wr::Vec3), image.size(), f);
     std::fwrite(albedo.data(), sizeof(wr::Vec3), albedo.size(), f);
+    std::fwrite(normal.data(), sizeof(wr::Vec3), normal.size(), f);
+    std::fwrite(denoised.data(), sizeof(wr::Vec3), denoised.size(), f);
     std::fclose(f);
     std::printf("paths=%llu rays=%llu threw=%d\n", (unsigned long long)renderer->lastStats().paths,
                 (unsigned long long)renderer->lastStats().extensionRays, threw ? 1 : 0);

@@ -37,10 +37,18 @@ def test_cpp_main_matches_python_and_oracle(gpu, oracle, tmp_path):
     out = tmp_path / "img.bin"
     r = subprocess.run([str(exe), str(out)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
-    data = np.fromfile(out, np.float32).reshape(2, 48, 48, 3)
+    data = np.fromfile(out, np.float32).reshape(4, 48, 48, 3)
     sd = _cpp_scene()
     py = gpu.Renderer(capacity=1 << 14).render(gpu.Scene.from_data(sd))
     np.testing.assert_allclose(data[0], py.rgb, rtol=1e-5, atol=1e-6)
     np.testing.assert_allclose(data[1], py.albedo, rtol=1e-6, atol=1e-7)
     o = oracle.scene(sd).render()[0]
     np.testing.assert_allclose(data[0], o, rtol=2e-3, atol=2e-4)
+    # denoise = true in the legacy call: the learned denoiser with the committed weights
+    # (found beside libwrk.so) applied to the same render
+    from offlinerenderer_b200 import denoise_train
+
+    dn = gpu.Denoiser()
+    denoise_train.load_weights(dn)
+    ref = dn.infer(data[0], data[1], data[2])
+    assert np.abs(np.log1p(data[3]) - np.log1p(ref)).max() < 1e-3
