@@ -41,6 +41,7 @@ struct FwdPlan {
     FwdShape shape;
     int chunk;
     uint32_t smem, grid;
+    bool halo;  // small-N kernel: resident weights, one halo load per 8 x 16 tile
 };
 struct WgradPlan {
     WgradShape shape;
@@ -53,10 +54,14 @@ int chunk_for(uint32_t channels);
 // as a 2-D [rows][K] bf16 matrix (box = boxK x boxRows).  Return 0 on success.
 int make_act_map(CUtensorMap* m, const void* base, uint32_t C, uint32_t W, uint32_t H, uint32_t B, uint32_t boxC);
 int make_weight_map(CUtensorMap* m, const void* base, uint32_t K, uint32_t rows, uint32_t boxK, uint32_t boxRows);
-int plan_fwd(uint32_t B, uint32_t H, uint32_t W, uint32_t Cin, uint32_t N, FwdPlan* p);
+int plan_fwd(uint32_t B, uint32_t H, uint32_t W, uint32_t Cin, uint32_t N, uint32_t numSMs, FwdPlan* p);
 int plan_wgrad(uint32_t B, uint32_t H, uint32_t W, uint32_t Cin, uint32_t Cout, uint32_t numSMs, WgradPlan* p);
-cudaError_t launch_fwd(const FwdPlan& p, const CUtensorMap& mx, const CUtensorMap& mw, const Epilogue& ep,
-                       uint32_t* err, cudaStream_t st);
+// Input tensor map for a forward plan (tiled or halo boxes); 0 on success.  The halo
+// kernel reads the weights straight from memory: its `mw` is not used, so only the
+// tiled kernel needs make_weight_map.
+int make_input_map(const FwdPlan& p, const void* x, CUtensorMap* mx);
+cudaError_t launch_fwd(const FwdPlan& p, const CUtensorMap& mx, const CUtensorMap& mw, const void* w,
+                       const Epilogue& ep, uint32_t* err, cudaStream_t st);
 cudaError_t launch_wgrad(const WgradPlan& p, const CUtensorMap& mg, const CUtensorMap& mx, float* dW, uint32_t* err,
                          cudaStream_t st);
 

@@ -439,11 +439,11 @@ int set_shape(wrk_denoiser* d, uint32_t B, uint32_t H, uint32_t W) {
         const LayerDef& L = kDefs[i];
         const uint32_t h = lvl_h(d, L.level), w = lvl_w(d, L.level), coPad = pad16(L.cout);
         IO io = layer_io(d, i);
-        if (conv::plan_fwd(B, h, w, L.cin, coPad, &d->fplan[i]))
+        if (conv::plan_fwd(B, h, w, L.cin, coPad, d->numSMs, &d->fplan[i]))
             return dfail(WRK_ERR_INVALID, "no forward plan for layer %d", i);
         int ch = d->fplan[i].chunk;
-        if (conv::make_act_map(&d->fin[i], io.in, L.cin, w, h, B, ch) ||
-            conv::make_weight_map(&d->fw[i], d->wf[i].p, 9 * L.cin, coPad, ch, coPad))
+        if (conv::make_input_map(d->fplan[i], io.in, &d->fin[i]) ||
+            (!d->fplan[i].halo && conv::make_weight_map(&d->fw[i], d->wf[i].p, 9 * L.cin, coPad, ch, coPad)))
             return dfail(WRK_ERR_CUDA, "tensor map encoding failed (layer %d)", i);
         // weight gradient: G = g[i] (coPad channels), X = layer input
         if (conv::plan_wgrad(B, h, w, L.cin, coPad, d->numSMs, &d->wplan[i]))
@@ -457,14 +457,14 @@ int set_shape(wrk_denoiser* d, uint32_t B, uint32_t H, uint32_t W) {
             d->dsplit[i] = L.cin > 256 ? 2 : 1;
             uint32_t n = L.cin / d->dsplit[i];
             for (uint32_t s = 0; s < d->dsplit[i]; ++s) {
-                if (conv::plan_fwd(B, h, w, coPad, n, &d->dplan[i][s]))
+                if (conv::plan_fwd(B, h, w, coPad, n, d->numSMs, &d->dplan[i][s]))
                     return dfail(WRK_ERR_INVALID, "no data-gradient plan for layer %d", i);
                 d->dplan[i][s].shape.wRow0 = s * n;
                 int dc = d->dplan[i][s].chunk;
-                if (conv::make_weight_map(&d->dwmap[i][s], d->wd[i].p, 9 * coPad, L.cin, dc, n))
+                if (!d->dplan[i][s].halo && conv::make_weight_map(&d->dwmap[i][s], d->wd[i].p, 9 * coPad, L.cin, dc, n))
                     return dfail(WRK_ERR_CUDA, "tensor map encoding failed (layer %d dgrad)", i);
             }
-            if (conv::make_act_map(&d->din[i], d->g[i].p, coPad, w, h, B, d->dplan[i][0].chunk))
+            if (conv::make_input_map(d->dplan[i][0], d->g[i].p, &d->din[i]))
                 return dfail(WRK_ERR_CUDA, "tensor map encoding failed (layer %d dgrad input)", i);
         }
     }
@@ -484,7 +484,7 @@ int conv_forward(wrk_denoiser* d, int i) {
     ep.coutValid = i == kLayers - 1 ? 16u : L.cout;  // head: padded channels are written as zero
     ep.relu = L.relu;
     ep.outF32 = i == kLayers - 1;
-    DCK(conv::launch_fwd(d->fplan[i], d->fin[i], d->fw[i], ep, d->err.as<uint32_t>(), d->stream));
+    DCK(conv::launch_fwd(d->fplan[i], d->fin[i], d->fw[i], d->wf[i].p, ep, d->err.as<uint32_t>(), d->stream));
     return WRK_OK;
 }
 
@@ -581,7 +581,8 @@ int backward(wrk_denoiser* d) {
                 ep.outOffset = s * n;
                 ep.outF32 = 1;
             }
-            DCK(conv::launch_fwd(d->dplan[i][s], d->din[i], d->dwmap[i][s], ep, d->err.as<uint32_t>(), d->stream));
+            DCK(conv::launch_fwd(d->dplan[i][s], d->din[i], d->dwmap[i][s], d->wd[i].p, ep, d->err.as<uint32_t>(),
+                                 d->stream));
         }
         // combine kernels that produce the G of the layer below
         const uint32_t catC[3] = {96, 192, 384};
@@ -677,9 +678,11 @@ int wrk_conv3x3_forward(const void* x, uint32_t B, uint32_t H, uint32_t W, uint3
     if (err.alloc(4)) return dfail(WRK_ERR_CUDA, "allocation failed");
     DCK(cudaMemset(err.p, 0, 4));
     conv::FwdPlan plan;
-    if (conv::plan_fwd(B, H, W, Cin, N, &plan)) return dfail(WRK_ERR_INVALID, "no conv plan");
+    if (conv::plan_fwd(B, H, W, Cin, N, (uint32_t)sms, &plan)) return dfail(WRK_ERR_INVALID, "no conv plan");
     CUtensorMap mx, mw;
-    if (conv::make_act_map(&mx, x, Cin, W, H, B, plan.chunk) || conv::make_weight_map(&mw, wp, 9 * Cin, N, plan.chunk, N))
+    memset(&mw, 0, sizeof(mw));
+    if (conv::make_input_map(plan, x, &mx) ||
+        (!plan.halo && conv::make_weight_map(&mw, wp, 9 * Cin, N, plan.chunk, N)))
         return dfail(WRK_ERR_CUDA, "tensor map encoding failed (pointers must be 16-byte aligned)");
     Epilogue ep{};
     ep.bias = bias;
@@ -689,7 +692,7 @@ int wrk_conv3x3_forward(const void* x, uint32_t B, uint32_t H, uint32_t W, uint3
     ep.coutValid = Cout;
     ep.relu = flags & 1u;
     ep.outF32 = (flags >> 1) & 1u;
-    DCK(conv::launch_fwd(plan, mx, mw, ep, err.as<uint32_t>(), 0));
+    DCK(conv::launch_fwd(plan, mx, mw, wp, ep, err.as<uint32_t>(), 0));
     uint32_t e = 0;
     DCK(cudaMemcpy(&e, err.p, 4, cudaMemcpyDeviceToHost));
     if (e) return dfail(WRK_ERR_DEVICE, "conv kernel timed out (flags 0x%x)", e);
