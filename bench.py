@@ -191,6 +191,48 @@ def served_legs(args, rend, local):
     return out
 
 
+def batched_scenes_leg(local):
+    """64 Cornell variants (own scene each: rotated boxes, 0-8 icospheres, 1k-60k
+    triangles), resolutions 128^2-1024^2 and 4-256 spp, submitted together to one
+    server: every request's paths share the wavefront queues, every path finds its
+    scene through its request (multi-scene kernels), one captured graph per chunk.
+    Launch shape from the autotuner on one of the requests."""
+    import torch
+
+    from offlinerenderer_b200 import wrk
+
+    t0 = time.perf_counter()
+    sds = [scenes.cornell_variant(k) for k in range(64)]
+    scs = [wrk.Scene.from_data(sd, device=local) for sd in sds]
+    build_s = time.perf_counter() - t0
+    tune = wrk.autotune(scs[1], device=local)
+    srv = wrk.Server(device=local, capacity=tune["capacity"], chunk=tune["chunk"], shade_block=tune["shadeBlock"],
+                     pool_bytes=8 << 30)
+    srv.wait(srv.submit(scs[0], settings=scenes.RenderSettings(64, 64, 1)))  # graph capture
+    out = torch.empty((1024 * 1024 * 3,), dtype=torch.float32, device=f"cuda:{local}")
+    for t in list(srv._shapes):
+        srv.result_device(t, out.data_ptr())
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    pending = [srv.submit(sc) for sc in scs]
+    gpu_ms, steps = 0.0, 0
+    while pending:
+        st = srv.step()
+        steps += 1
+        gpu_ms += st["lastChunkMs"]
+        for t in [t for t in pending if srv.ready(t)]:
+            srv.result_device(t, out.data_ptr())
+            pending.remove(t)
+    wall = time.perf_counter() - t1
+    samples = sum(sd.settings.width * sd.settings.height * sd.settings.spp for sd in sds)
+    tris = [sd.num_triangles for sd in sds]
+    return {"workload": "64 Cornell variants, 1 scene each (rotated boxes, 0-8 icospheres subdiv 2-5), "
+                        "128^2-1024^2, 4-256 spp, one server",
+            "samples": samples, "triangles_min": min(tris), "triangles_max": max(tris), "scene_build_s": build_s,
+            "wall_ms": wall * 1e3, "gpu_ms": gpu_ms, "steps": steps, "msamples_per_s": samples / wall / 1e6,
+            "autotune": {k: tune[k] for k in ("capacity", "chunk", "shadeBlock", "bestMs")}}
+
+
 def cpu_reference_rate(sd, threads: int, target_s: float = 12.0):
     """Reference shading code on the host cores (oracle/_ref), bounded sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -378,6 +420,7 @@ def main():
     served = {}
     if rank == 0 and world == 1 and not args.no_served:
         served = served_legs(args, rend, local)
+        served["batched_scenes"] = batched_scenes_leg(local)
 
     if rank == 0:
         out = {

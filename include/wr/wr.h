@@ -2,6 +2,7 @@
 #pragma once
 
 #include "wr/context.h"
+#include "wr/image.h"
 #include "wr/renderer.h"
 #include "wr/scene.h"
 #include "wr/types.h"

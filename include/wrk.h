@@ -273,6 +273,11 @@ int wrk_camera_rays(const wrk_camera* cam, uint32_t width, uint32_t height, cons
                     const uint32_t* d_samples, uint32_t n, uint32_t seed, float* d_rays);
 /* Exposure 2.2, ACES filmic fit, gamma 1/2.2, 8-bit (libWR/test/helpers/image.cpp:14-49). */
 int wrk_tonemap_aces(const float* d_rgb, uint32_t numPixels, uint8_t* d_out);
+/* savePNG of libWR's test layer (libWR/test/helpers/image.cpp:23-49): host float RGB
+ * (width*height*3) tone mapped on the GPU as above and written as an 8-bit RGB PNG. */
+int wrk_image_save_png(const char* path, const float* rgb, uint32_t width, uint32_t height);
+/* Writes host RGB8 bytes (width*height*3) as a PNG file (zlib deflate); 0 on success. */
+int wrk_png_write(const char* path, const uint8_t* rgb8, uint32_t width, uint32_t height);
 
 /* ---- learned denoiser: replaces the OptiX AI denoiser of libWR
  *      (libWR/src/internal/denoiser.cpp:17-195: optixDenoiserCreate :30-35,

@@ -269,9 +269,14 @@ constexpr uint32_t kHaloW = 10, kHaloH = 18, kHaloPix = kHaloW * kHaloH, kHTileW
 // destination stays 128-byte aligned
 constexpr uint32_t kHaloGroupBytes = 2944;
 
+// CIN > 0: the input channel count is a compile-time constant, so the MMA issuer's
+// 9 x CIN/16 descriptors are fixed offsets from one base descriptor per tile
+// (0 = read sh.Cin at run time).
+template <int CIN>
 __global__ void __launch_bounds__(192, 1)
     k_conv_fwd_halo(const __grid_constant__ CUtensorMap mh, const __nv_bfloat16* __restrict__ wgt, FwdShape sh,
                     Epilogue ep, uint32_t* err) {
+    if (CIN > 0) sh.Cin = CIN;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const uint32_t G = sh.Cin / 8;                      // channel groups
@@ -363,15 +368,20 @@ __global__ void __launch_bounds__(192, 1)
                 }
                 tc_fence_after();
                 const uint32_t acc = tmem + buf * sh.N;
-                const uint32_t h = base + s * stageBytes;
-                uint32_t first = 1;
+                // descriptors advance by (byte offset >> 4) in their low 14-bit address field
+                const uint64_t a0 = sdesc(base + s * stageBytes, lboA, sboA, 0);
+                const uint64_t b0 = sdesc(wbase, lboB, sboB, 0);
+                const uint32_t nUnits = sh.N;  // lboB >> 4
+                constexpr uint32_t kKC = CIN > 0 ? CIN / 16 : 8;
+#pragma unroll
                 for (uint32_t tap = 0; tap < 9; ++tap) {
-                    const uint32_t shift = ((tap / 3) * kHaloW + (tap % 3)) * 16;
-                    for (uint32_t kk = 0; kk < sh.Cin / 16; ++kk) {
-                        const uint64_t ad = sdesc(h + 2 * kk * lboA + shift, lboA, sboA, 0);
-                        const uint64_t bd = sdesc(wbase + ((tap * sh.Cin + 16 * kk) / 8) * lboB, lboB, sboB, 0);
-                        umma_bf16(acc, ad, bd, idesc, first ? 0u : 1u);
-                        first = 0;
+                    const uint32_t shift = ((tap / 3) * kHaloW + (tap % 3));  // 16-byte units
+#pragma unroll
+                    for (uint32_t kk = 0; kk < kKC; ++kk) {
+                        if (CIN == 0 && kk >= sh.Cin / 16) break;
+                        const uint64_t ad = a0 + (2 * kk * (kHaloGroupBytes >> 4) + shift);
+                        const uint64_t bd = b0 + ((tap * sh.Cin + 16 * kk) / 8) * nUnits;
+                        umma_bf16(acc, ad, bd, idesc, (tap | kk) ? 1u : 0u);
                     }
                 }
                 umma_commit(empty(s));
@@ -703,9 +713,23 @@ cudaError_t launch_fwd(const FwdPlan& p, const CUtensorMap& mx, const CUtensorMa
                        const Epilogue& ep, uint32_t* err, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
     if (p.halo) {
-        e = set_smem(k_conv_fwd_halo, p.smem);
-        if (e == cudaSuccess)
-            k_conv_fwd_halo<<<p.grid, 192, p.smem, st>>>(mx, (const __nv_bfloat16*)w, p.shape, ep, err);
+        const __nv_bfloat16* wb = (const __nv_bfloat16*)w;
+#define WRK_HALO_CASE(C)                                                                       \
+    case C:                                                                                    \
+        e = set_smem(k_conv_fwd_halo<C>, p.smem);                                             \
+        if (e == cudaSuccess) k_conv_fwd_halo<C><<<p.grid, 192, p.smem, st>>>(mx, wb, p.shape, ep, err); \
+        break;
+        switch (p.shape.Cin) {
+            WRK_HALO_CASE(16)
+            WRK_HALO_CASE(32)
+            WRK_HALO_CASE(64)
+            WRK_HALO_CASE(96)
+            default:
+                e = set_smem(k_conv_fwd_halo<0>, p.smem);
+                if (e == cudaSuccess) k_conv_fwd_halo<0><<<p.grid, 192, p.smem, st>>>(mx, wb, p.shape, ep, err);
+                break;
+        }
+#undef WRK_HALO_CASE
         return e != cudaSuccess ? e : cudaGetLastError();
     }
     switch (p.chunk) {

@@ -19,6 +19,7 @@
 #include <string>
 #include <vector>
 
+#include "../../include/wr/image.h"
 #include "../../include/wr/wr.h"
 #include "../../include/wrk.h"
 
@@ -480,3 +481,88 @@ void Renderer::render(Scene* scene, const Camera& camera, Vec3* out, uint32_t wi
 }
 
 }  // namespace wr
+
+// ---------------------------------------------------------------------------
+// PNG output (test_helpers::savePNG, libWR/test/helpers/image.cpp:23-49)
+namespace wrk {
+int report_error(int code, const char* msg);
+}
+
+namespace {
+
+void put_be32(std::vector<uint8_t>& o, uint32_t v) {
+    o.push_back((uint8_t)(v >> 24));
+    o.push_back((uint8_t)(v >> 16));
+    o.push_back((uint8_t)(v >> 8));
+    o.push_back((uint8_t)v);
+}
+
+void put_chunk(std::vector<uint8_t>& o, const char* type, const uint8_t* data, size_t n) {
+    put_be32(o, (uint32_t)n);
+    const size_t start = o.size();
+    o.insert(o.end(), type, type + 4);
+    if (n) o.insert(o.end(), data, data + n);
+    uLong crc = crc32(0L, Z_NULL, 0);
+    crc = crc32(crc, o.data() + start, (uInt)(o.size() - start));
+    put_be32(o, (uint32_t)crc);
+}
+
+}  // namespace
+
+extern "C" int wrk_png_write(const char* path, const uint8_t* rgb8, uint32_t width, uint32_t height) {
+    if (!path || !rgb8 || width == 0 || height == 0) return wrk::report_error(WRK_ERR_INVALID, "png: bad arguments");
+    std::vector<uint8_t> raw((size_t)height * (1 + 3 * (size_t)width));
+    for (uint32_t y = 0; y < height; ++y) {
+        uint8_t* row = raw.data() + (size_t)y * (1 + 3 * (size_t)width);
+        row[0] = 0;  // filter: none
+        std::memcpy(row + 1, rgb8 + (size_t)y * 3 * width, 3 * (size_t)width);
+    }
+    uLongf zlen = compressBound((uLong)raw.size());
+    std::vector<uint8_t> z(zlen);
+    if (compress2(z.data(), &zlen, raw.data(), (uLong)raw.size(), 6) != Z_OK)
+        return wrk::report_error(WRK_ERR_INVALID, "png: deflate failed");
+    std::vector<uint8_t> png = {0x89, 'P', 'N', 'G', 0x0d, 0x0a, 0x1a, 0x0a};
+    uint8_t ihdr[13];
+    for (int k = 0; k < 4; ++k) {
+        ihdr[k] = (uint8_t)(width >> (24 - 8 * k));
+        ihdr[4 + k] = (uint8_t)(height >> (24 - 8 * k));
+    }
+    ihdr[8] = 8;   // bit depth
+    ihdr[9] = 2;   // colour type RGB
+    ihdr[10] = 0;  // deflate
+    ihdr[11] = 0;  // adaptive filtering
+    ihdr[12] = 0;  // no interlace
+    put_chunk(png, "IHDR", ihdr, 13);
+    put_chunk(png, "IDAT", z.data(), zlen);
+    put_chunk(png, "IEND", nullptr, 0);
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return wrk::report_error(WRK_ERR_INVALID, (std::string("png: cannot open ") + path).c_str());
+    const bool ok = std::fwrite(png.data(), 1, png.size(), f) == png.size();
+    std::fclose(f);
+    return ok ? WRK_OK : wrk::report_error(WRK_ERR_INVALID, "png: write failed");
+}
+
+extern "C" int wrk_image_save_png(const char* path, const float* rgb, uint32_t width, uint32_t height) {
+    if (!path || !rgb || width == 0 || height == 0) return wrk::report_error(WRK_ERR_INVALID, "png: bad arguments");
+    const size_t np = (size_t)width * height;
+    void* d = nullptr;
+    int dev = 0, n = 0;
+    if (wrk_device_count(&n) || n == 0) return wrk::report_error(WRK_ERR_NO_DEVICE, "no CUDA device available");
+    int rc = wrk_malloc(dev, np * 12 + np * 3 + 16, &d);
+    if (rc) return rc;
+    float* df = static_cast<float*>(d);
+    uint8_t* db = reinterpret_cast<uint8_t*>(df + 3 * np);
+    std::vector<uint8_t> bytes(np * 3);
+    if (!(rc = wrk_memcpy_htod(df, rgb, np * 12)) && !(rc = wrk_tonemap_aces(df, (uint32_t)np, db)))
+        rc = wrk_memcpy_dtoh(bytes.data(), db, np * 3);
+    wrk_free(d);
+    if (rc) return rc;
+    return wrk_png_write(path, bytes.data(), width, height);
+}
+
+namespace test_helpers {
+void savePNG(const char* filename, const wr::Vec3* image, uint32_t width, uint32_t height) {
+    int rc = wrk_image_save_png(filename, reinterpret_cast<const float*>(image), width, height);
+    if (rc) throw std::runtime_error(std::string("savePNG(") + (filename ? filename : "") + "): " + wrk_last_error());
+}
+}  // namespace test_helpers

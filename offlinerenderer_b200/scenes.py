@@ -389,3 +389,51 @@ def scale_test(width=1920, height=1080, spp=64, seed=1, grid=1024, spheres=250, 
     return b.build(env=(0.12, 0.12, 0.15), camera=cam,
                    settings=RenderSettings(width, height, spp, maxBounces=8, russianRouletteDepth=3.0, seed=seed),
                    name=f"scale_{width}x{height}_{spp}spp")
+
+
+def _random_material(b: _Builder, rng):
+    """One of the five BSDF kinds, parameters drawn as in the scale test."""
+    kind = int(rng.integers(0, 5))
+    alb = tuple(rng.uniform(0.1, 0.9, 3))
+    if kind == 0:
+        return b.lambertian(alb)
+    if kind == 1:
+        return b.glass((0.999, 0.999, 0.999), float(rng.uniform(1.3, 1.7)))
+    if kind == 2:
+        return b.ggx(alb, float(rng.uniform(0.05, 0.8)), 1.0)
+    if kind == 3:
+        return b.ggx(alb, float(rng.uniform(0.05, 0.8)), 0.0)
+    return b.ggx_transmission((0.999, 0.999, 0.999), float(rng.uniform(0.05, 0.8)), float(rng.uniform(1.3, 1.7)))
+
+
+def cornell_variant(seed: int, max_tris: int = 60000) -> SceneData:
+    """One scene of the batched-scenes workload: the Cornell room with both boxes
+    rotated by U(-45, 45) degrees and 0-8 icospheres (subdivision 2-5, random
+    materials as in the scale test), the subdivision lowered where needed to keep
+    the scene within `max_tris`; resolution from {128^2, 256^2, 512^2, 1024^2} and
+    spp from {4, 16, 64, 256}, both drawn from the seed."""
+    rng = np.random.default_rng(10_000 + seed)
+    b = _Builder()
+    white = b.lambertian((0.73, 0.73, 0.73))
+    red = b.lambertian((0.63, 0.065, 0.05))
+    green = b.lambertian((0.14, 0.45, 0.09))
+    light = b.emissive((17.0, 12.0, 4.0))
+    _room(b, white, red, green, light)
+    _box(b, 0.66, 0.64, 0.3, 0.6, 0.3, float(rng.uniform(-45, 45)), white)
+    _box(b, 0.34, 0.36, 0.3, 0.3, 0.3, float(rng.uniform(-45, 45)), white)
+    tris = 36
+    for _ in range(int(rng.integers(0, 9))):
+        sub = int(rng.integers(2, 6))
+        while sub > 2 and tris + 20 * 4 ** sub > max_tris:
+            sub -= 1
+        if tris + 20 * 4 ** sub > max_tris:
+            break
+        r = float(rng.uniform(0.05, 0.12))
+        c = (float(rng.uniform(0.15, 0.85)), float(rng.uniform(0.05, 0.7)) + r, float(rng.uniform(0.15, 0.85)))
+        _sphere(b, c, r, sub, _random_material(b, rng))
+        tris += 20 * 4 ** sub
+    res = int(rng.choice([128, 256, 512, 1024]))
+    spp = int(rng.choice([4, 16, 64, 256]))
+    return b.build(camera=_cornell_camera(res, res),
+                   settings=RenderSettings(res, res, spp, maxBounces=8, russianRouletteDepth=3.0, seed=seed + 1),
+                   name=f"cornell_variant_{seed}")

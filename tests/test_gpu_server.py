@@ -146,3 +146,19 @@ def test_autotune_picks_a_listed_shape(gpu, world):
     assert len(res["trials"]) == 18
     best = min(res["trials"], key=lambda t: t["ms"])
     assert (res["capacity"], res["chunk"], res["shadeBlock"]) == (best["capacity"], best["chunk"], best["shadeBlock"])
+
+
+def test_batched_variant_scenes_each_as_alone(gpu):
+    """Batched scenes in one launch: Cornell variants, each its own scene (own BVH,
+    materials, lights), rendered together; each image equals its solo render."""
+    sds = [scenes.cornell_variant(k) for k in range(6)]
+    scs = [gpu.Scene.from_data(sd) for sd in sds]
+    sts = [_settings(48, 32, 4, sd.settings) for sd in sds]
+    srv = gpu.Server(capacity=1 << 14)
+    tickets = [srv.submit(sc, settings=st) for sc, st in zip(scs, sts)]
+    for t in tickets:
+        srv.wait(t)
+    for t, sc, st in zip(tickets, scs, sts):
+        rgb, alb, nrm, _ = srv.result(t)
+        solo = _solo(gpu, sc, sc._data.camera, st)
+        assert _close(rgb, solo.rgb) and _close(nrm, solo.normal)
