@@ -46,6 +46,7 @@ struct RenderParams {
     Vec3* normalOut = nullptr;      // first-hit normal guide, averaged over spp
     bool rawGuides = false;         // guides as per-pixel sums (libWR's buffers)
     uint32_t maxIterations = 8;     // wavefront iterations per path (8 = libWR's host loop)
+    bool useEnvironmentMap = false; // misses read Scene::setEnvironmentMap's map (libWR: uniform only)
 };
 
 struct RenderStats {

@@ -71,6 +71,12 @@ typedef struct {
 #define WRK_FLAG_STAGE_TIMING 2u
 /* Served requests: pass the result through the server's learned denoiser. */
 #define WRK_FLAG_DENOISE 4u
+/* Rays that miss take their radiance from the scene's environment map (lat-long,
+ * bilinear, wrap in u, clamp in v: getEnvironmentRadiance of
+ * libWR/kernels/utils/environment_sampling.cuh:10-52).  libWR's own miss program
+ * adds only the uniform radiance (libWR/kernels/trace.cu:143-148), which stays the
+ * default. */
+#define WRK_FLAG_ENV_MAP 8u
 
 enum {
     WRK_STAGE_CONTROL = 0,
@@ -135,6 +141,9 @@ int wrk_scene_set_materials(wrk_scene* s, const wrk_material* materials, uint32_
 /* RGBA8 texture (Scene::loadTexture, scene.cpp:246-264); returns the 1-based id. */
 int wrk_scene_add_texture(wrk_scene* s, const uint8_t* rgba, uint32_t width, uint32_t height, uint32_t* outId);
 int wrk_scene_set_environment(wrk_scene* s, const float rgb[3]);
+/* Environment map (Scene::setEnvironmentMap, scene.cpp:289-348): width*height RGBA f32
+ * texels, row 0 = the +y pole (v = 0); kept on the device after finalize. */
+int wrk_scene_set_environment_map(wrk_scene* s, const float* rgba, uint32_t width, uint32_t height);
 /* Scene::finalize (scene.cpp:350-557): uploads, builds the emissive list and power
  * CDF (same serial FP32 order as scene.cpp:423-491), builds the 8-wide BVH on the GPU
  * (replaces optixAccelBuild, scene.cpp:493-550). */

@@ -121,7 +121,10 @@ struct wrk_scene {
     std::vector<std::vector<uint8_t>> tex;
     std::vector<uint32_t> texW, texH;
     float env[3] = {0, 0, 0};
+    std::vector<float> envMap;
+    uint32_t envW = 0, envH = 0;
     bool finalized = false;
+    DevBuf dEnvMap;
     DevBuf dVtx, dNrm, dUv, dIdx, dTriMat, dMats, dTexels, dTexInfo, dEmissive, dCdf, dErr;
     uint4* nodes = nullptr;
     float4* tris = nullptr;
@@ -459,6 +462,15 @@ int wrk_scene_set_environment(wrk_scene* s, const float rgb[3]) {
     return WRK_OK;
 }
 
+int wrk_scene_set_environment_map(wrk_scene* s, const float* rgba, uint32_t w, uint32_t h) {
+    if (!s || !rgba || w == 0 || h == 0) return fail(WRK_ERR_INVALID, "bad environment map arguments");
+    if (s->finalized) return fail(WRK_ERR_STATE, "scene already finalized");
+    s->envMap.assign(rgba, rgba + 4 * (size_t)w * h);
+    s->envW = w;
+    s->envH = h;
+    return WRK_OK;
+}
+
 int wrk_scene_finalize(wrk_scene* s) {
     if (!s) return fail(WRK_ERR_INVALID, "null scene");
     if (s->finalized) return WRK_OK;  // as Scene::finalize (scene.cpp:351)
@@ -519,6 +531,12 @@ int wrk_scene_finalize(wrk_scene* s) {
     v.nodes = s->nodes;
     v.tris = s->tris;
     v.numNodes = br.numNodes;
+    if (!s->envMap.empty()) {
+        if ((rc = upload(s->dEnvMap, s->envMap))) return rc;
+        v.envMap = s->dEnvMap.as<float4>();
+        v.envW = s->envW;
+        v.envH = s->envH;
+    }
     s->finalized = true;
     return WRK_OK;
 }
@@ -631,6 +649,7 @@ void fill_frame(Frame& f, const wrk_camera& cam, const wrk_render_params& p) {
     f.fireflyClamp = p.fireflyClamp;
     f.tilesX = (p.width % 8 == 0 && p.height % 4 == 0) ? p.width / 8 : 0;
     f.perSample = p.width * p.height;
+    f.flags = p.flags;
 }
 }  // namespace wrk
 

@@ -327,8 +327,10 @@ constexpr int kRefillAt = WRK_REFILL_AT;
 
 // Adds a miss's environment term and accumulates the path into its request's sums
 // (__miss__trace + the raygen miss branch, trace.cu:143-148).
-__device__ __forceinline__ void miss_accumulate(const float env[3], const Frame& f, float4 th, float4 rd) {
-    float3 L = make_float3(rd.x + th.x * env[0], rd.y + th.y * env[1], rd.z + th.z * env[2]);
+__device__ __forceinline__ void miss_accumulate(const DevScene& sc, const Frame& f, float4 th, float4 rd, float3 dir) {
+    float3 e = make_float3(sc.env[0], sc.env[1], sc.env[2]);
+    if ((f.flags & WRK_FLAG_ENV_MAP) && sc.envMap) e = env_lookup(sc.envMap, sc.envW, sc.envH, dir);
+    float3 L = make_float3(rd.x + th.x * e.x, rd.y + th.y * e.y, rd.z + th.z * e.z);
     L = clamp_fireflies(L, f.fireflyClamp);
     atomicAdd(f.accum + __float_as_uint(rd.w), make_float4(L.x, L.y, L.z, 0.0f));
 }
@@ -420,10 +422,10 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
                 if constexpr (kMulti) {
                     const DevScene& sc = q.scenes[sceneIdx];
                     if (t.pBest != kNoHit) bucket = t.mBest < sc.numMats ? bucket_of(sc.mats[t.mBest].type) : kBucketOther;
-                    else miss_accumulate(sc.env, f, th, rd);
+                    else miss_accumulate(sc, f, th, rd, make_float3(t.r.dx, t.r.dy, t.r.dz));
                 } else {
                     if (t.pBest != kNoHit) bucket = t.mBest < s0.numMats ? bucket_of(s0.mats[t.mBest].type) : kBucketOther;
-                    else miss_accumulate(s0.env, f, th, rd);
+                    else miss_accumulate(s0, f, th, rd, make_float3(t.r.dx, t.r.dy, t.r.dz));
                 }
                 missed = t.pBest == kNoHit;
             }

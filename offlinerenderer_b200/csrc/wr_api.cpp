@@ -332,6 +332,9 @@ void Scene::finalize(const SceneBuildConfig&) {
     }
     float env[3] = {s.env.x, s.env.y, s.env.z};
     check(wrk_scene_set_environment(s.handle, env), "wrk_scene_set_environment");
+    if (!s.envMap.empty())
+        check(wrk_scene_set_environment_map(s.handle, s.envMap.data(), s.envW, s.envH),
+              "wrk_scene_set_environment_map");
     check(wrk_scene_finalize(s.handle), "wrk_scene_finalize");
     check(wrk_scene_buffers_get(s.handle, &s.bufs), "wrk_scene_buffers_get");
     s.finalized = true;
@@ -419,7 +422,7 @@ void Renderer::render(Scene* scene, const Camera& camera, Vec3* out, const Rende
     rp.fireflyClamp = p.fireflyClamp;
     rp.seed = p.seed;
     rp.maxIterations = p.maxIterations;
-    rp.flags = p.rawGuides ? WRK_FLAG_RAW_GUIDES : 0u;
+    rp.flags = (p.rawGuides ? WRK_FLAG_RAW_GUIDES : 0u) | (p.useEnvironmentMap ? WRK_FLAG_ENV_MAP : 0u);
     wrk_render_stats st{};
     if (!p.denoiser.enabled) {
         check(wrk_render(m_impl->handle, scene->native(), &c, &rp, reinterpret_cast<float*>(out),

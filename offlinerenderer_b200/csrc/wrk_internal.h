@@ -80,6 +80,8 @@ struct DevScene {
     const uint4* nodes;
     const float4* tris;
     uint32_t numNodes;
+    const float4* envMap;  // lat-long RGBA f32 map (null = none); used with WRK_FLAG_ENV_MAP
+    uint32_t envW, envH;
 };
 
 // One queue's entries, SoA.  Fields a queue does not carry are null.
@@ -136,7 +138,7 @@ struct Frame {
     uint32_t spp, useNEE, maxBounces, seed, maxIter, sampleOffset;
     float rrStart, fireflyClamp;
     uint32_t scene;  // index into Queues::scenes
-    uint32_t pad;
+    uint32_t flags;  // WRK_FLAG_* of the request
     float4* accum;   // radiance sum per pixel
     float4* albedo;  // first-hit albedo sum per pixel
     float4* normal;  // first-hit normal sum per pixel

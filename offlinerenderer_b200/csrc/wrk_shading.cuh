@@ -236,6 +236,30 @@ __device__ __forceinline__ float4 tex_fetch(const uint8_t* __restrict__ px, uint
     return o;
 }
 
+// ---- environment map: directionToUV + a float4 texture with linear filtering,
+//      normalized coordinates, wrap in u and clamp in v
+//      (libWR/kernels/utils/environment_sampling.cuh:10-52, scene.cpp:325-331) ----
+__device__ __forceinline__ float3 env_lookup(const float4* __restrict__ map, uint32_t w, uint32_t h, float3 d) {
+    d = normalize(d);
+    float phi = atan2f(d.z, d.x);
+    float theta = acosf(fmaxf(-1.0f, fminf(1.0f, d.y)));
+    float u = (phi + 3.14159265f) / (2.0f * 3.14159265f);
+    float v = theta / 3.14159265f;
+    float x = (u - floorf(u)) * (float)w - 0.5f;
+    float y = fminf(fmaxf(v, 0.0f), 1.0f) * (float)h - 0.5f;
+    float fx = floorf(x), fy = floorf(y);
+    float ax = rintf((x - fx) * 256.0f) * (1.0f / 256.0f), ay = rintf((y - fy) * 256.0f) * (1.0f / 256.0f);
+    int ix = (int)fx, iy = (int)fy;
+    int x0 = ((ix % (int)w) + (int)w) % (int)w, x1 = (x0 + 1) % (int)w;
+    int y0 = min(max(iy, 0), (int)h - 1), y1 = min(max(iy + 1, 0), (int)h - 1);
+    float4 t00 = __ldg(map + (size_t)y0 * w + x0), t10 = __ldg(map + (size_t)y0 * w + x1);
+    float4 t01 = __ldg(map + (size_t)y1 * w + x0), t11 = __ldg(map + (size_t)y1 * w + x1);
+    float bx = 1.0f - ax, by = 1.0f - ay;
+    return f3((t00.x * bx + t10.x * ax) * by + (t01.x * bx + t11.x * ax) * ay,
+              (t00.y * bx + t10.y * ax) * by + (t01.y * bx + t11.y * ax) * ay,
+              (t00.z * bx + t10.z * ax) * by + (t01.z * bx + t11.z * ax) * ay);
+}
+
 // ---- ACES filmic + gamma (libWR/test/helpers/image.cpp:14-49) ----
 __device__ __forceinline__ uint8_t aces_byte(float lin) {
     float x = lin * 2.2f;

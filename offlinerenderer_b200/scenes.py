@@ -77,6 +77,7 @@ class SceneData:
     uvs: np.ndarray | None = None  # (V,2) f32
     textures: list = dataclasses.field(default_factory=list)  # (H,W,4) u8, id = index+1
     env: tuple = (0.0, 0.0, 0.0)
+    env_map: np.ndarray | None = None  # (H, W, 4) f32 lat-long map, row 0 = +y pole
     camera: Camera | None = None
     settings: RenderSettings | None = None
     name: str = ""

@@ -22,6 +22,7 @@ LIB_PATH = os.path.join(HERE, "libwrk.so")
 
 WRK_FLAG_RAW_GUIDES = 1
 WRK_FLAG_STAGE_TIMING = 2
+WRK_FLAG_ENV_MAP = 8
 STAGES = ["control", "generate", "trace_extension", "trace_shadow", "shade_lambert", "shade_dielectric", "shade_ggx",
           "shade_emissive", "shade_lambert_resume"]
 BUCKETS = ["lambert", "dielectric", "ggx", "other", "lambert_resume"]
@@ -107,6 +108,7 @@ SIGNATURES = {
     "wrk_scene_set_materials": ([_VP, _VP, _U32], _I),
     "wrk_scene_add_texture": ([_VP, _VP, _U32, _U32, C.POINTER(_U32)], _I),
     "wrk_scene_set_environment": ([_VP, _VP], _I),
+    "wrk_scene_set_environment_map": ([_VP, _VP, _U32, _U32], _I),
     "wrk_scene_finalize": ([_VP], _I),
     "wrk_scene_bvh_info": ([_VP, C.POINTER(BvhInfoC)], _I),
     "wrk_scene_light_cdf": ([_VP, _VP, _VP, _U32, C.POINTER(_U32)], _I),
@@ -227,7 +229,7 @@ def camera_struct(cam) -> CameraC:
 
 
 def params_struct(st, spp=None, max_iterations=8, raw_guides=False, seed=None, sample_offset=0,
-                  stage_timing=False) -> RenderParamsC:
+                  stage_timing=False, env_map=False) -> RenderParamsC:
     p = RenderParamsC()
     p.width, p.height = st.width, st.height
     p.spp = st.spp if spp is None else spp
@@ -237,7 +239,8 @@ def params_struct(st, spp=None, max_iterations=8, raw_guides=False, seed=None, s
     p.fireflyClamp = st.fireflyClamp
     p.seed = st.seed if seed is None else seed
     p.maxIterations = max_iterations
-    p.flags = (WRK_FLAG_RAW_GUIDES if raw_guides else 0) | (WRK_FLAG_STAGE_TIMING if stage_timing else 0)
+    p.flags = ((WRK_FLAG_RAW_GUIDES if raw_guides else 0) | (WRK_FLAG_STAGE_TIMING if stage_timing else 0)
+               | (WRK_FLAG_ENV_MAP if env_map else 0))
     p.sampleOffset = sample_offset
     return p
 
@@ -291,6 +294,11 @@ class Scene:
     def setEnvironmentRadiance(self, rgb) -> None:
         self._env = tuple(float(x) for x in rgb)
 
+    def setEnvironmentMap(self, rgba: np.ndarray) -> None:
+        """(H, W, 4) float lat-long map (Scene::setEnvironmentMap takes a .hdr path;
+        the decoded texels are passed here); used by renders with env_map=True."""
+        self._env_map = np.ascontiguousarray(rgba, np.float32)
+
     @classmethod
     def from_data(cls, sd: "_scenes.SceneData", device: int = 0) -> "Scene":
         s = cls(device)
@@ -303,7 +311,7 @@ class Scene:
             return
         if not self._b.v:
             raise WrkError(1, "Scene has no geometry")
-        sd = self._b.build(env=self._env)
+        sd = self._b.build(env=self._env, env_map=getattr(self, "_env_map", None))
         self._data = sd
         self._finalize_data(sd)
 
@@ -328,6 +336,9 @@ class Scene:
             _check(L.wrk_scene_add_texture(self.handle, t.ctypes.data, t.shape[1], t.shape[0], C.byref(tid)))
         env = np.asarray(sd.env, np.float32)
         _check(L.wrk_scene_set_environment(self.handle, env.ctypes.data))
+        if sd.env_map is not None:
+            em = np.ascontiguousarray(sd.env_map, np.float32)
+            _check(L.wrk_scene_set_environment_map(self.handle, em.ctypes.data, em.shape[1], em.shape[0]))
         _check(L.wrk_scene_finalize(self.handle))
 
     def __del__(self):
@@ -410,12 +421,12 @@ class Renderer:
         _check(lib().wrk_renderer_set_launch(self.handle, chunk, shade_block))
 
     def render(self, scene: Scene, camera=None, settings=None, spp=None, guides=True, raw_guides=False,
-               max_iterations=8, seed=None, sample_offset=0, stage_timing=False) -> RenderResult:
+               max_iterations=8, seed=None, sample_offset=0, stage_timing=False, env_map=False) -> RenderResult:
         """Synchronous render into host buffers (rgb = sum/spp, as libWR returns it)."""
         cam = camera_struct(camera or scene._data.camera)
         st = settings or scene._data.settings
         p = params_struct(st, spp=spp, max_iterations=max_iterations, raw_guides=raw_guides, seed=seed,
-                          sample_offset=sample_offset, stage_timing=stage_timing)
+                          sample_offset=sample_offset, stage_timing=stage_timing, env_map=env_map)
         shape = (st.height, st.width, 3)
         rgb = np.zeros(shape, np.float32)
         alb = np.zeros(shape, np.float32) if guides else None

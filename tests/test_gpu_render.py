@@ -159,3 +159,43 @@ def test_sample_offset_split_equals_full_render(gpu):
     full = r.render(s, spp=8).rgb
     np.testing.assert_allclose((a + b) * 0.5, full, rtol=1e-5, atol=1e-6)
     assert np.abs(a - b).max() > 1e-3
+
+
+def test_environment_map_on_miss(gpu, oracle):
+    """WRK_FLAG_ENV_MAP: a camera ray that misses returns the environment map's
+    bilinear lat-long lookup of its direction (environment_sampling.cuh:10-52:
+    u = (atan2(z, x) + pi) / 2pi, v = acos(y) / pi; wrap in u, clamp in v); without
+    the flag the miss adds the uniform radiance, as libWR's miss program does."""
+    from offlinerenderer_b200 import scenes
+
+    H, W = 32, 64
+    yy, xx = np.mgrid[0:H, 0:W].astype(np.float32)
+    em = np.stack([0.5 + 0.4 * np.sin(xx / W * 2 * np.pi), 0.2 + yy / H, 0.1 + 0.3 * xx / W,
+                   np.ones_like(xx)], -1).astype(np.float32)
+    b = scenes._Builder()
+    m = b.lambertian((0.5, 0.5, 0.5))
+    b.mesh([[10, 10, 10], [10.01, 10, 10], [10, 10.01, 10]], [0, 1, 2], m)  # far away: every ray misses
+    cam = scenes.Camera(position=(0.0, 0.0, 0.0), target=(0.3, 0.4, 1.0), fovY=float(scenes._radians(90.0)),
+                        aspect=1.0)
+    sd = b.build(env=(0.25, 0.5, 0.75), env_map=em, camera=cam, settings=scenes.RenderSettings(24, 24, 1))
+    scene = gpu.Scene.from_data(sd)
+    r = gpu.Renderer(capacity=1 << 12)
+    plain = r.render(scene)
+    assert np.allclose(plain.rgb, np.array([0.25, 0.5, 0.75], np.float32))
+    lit = r.render(scene, env_map=True)
+    rays = gpu.camera_rays(cam, 24, 24, np.arange(24 * 24), np.zeros(24 * 24), 0)
+    d = rays[:, 4:7].astype(np.float64)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    u = (np.arctan2(d[:, 2], d[:, 0]) + np.pi) / (2 * np.pi)
+    v = np.arccos(np.clip(d[:, 1], -1, 1)) / np.pi
+    x, y = (u - np.floor(u)) * W - 0.5, np.clip(v, 0, 1) * H - 0.5
+    fx, fy = np.floor(x), np.floor(y)
+    ax, ay = np.rint((x - fx) * 256) / 256, np.rint((y - fy) * 256) / 256
+    x0 = fx.astype(int) % W
+    x1 = (x0 + 1) % W
+    y0, y1 = np.clip(fy.astype(int), 0, H - 1), np.clip(fy.astype(int) + 1, 0, H - 1)
+    ref = (((em[y0, x0] * (1 - ax)[:, None] + em[y0, x1] * ax[:, None]) * (1 - ay)[:, None])
+           + ((em[y1, x0] * (1 - ax)[:, None] + em[y1, x1] * ax[:, None]) * ay[:, None]))[:, :3]
+    # f32 atan2 / acos on the device vs f64 here can move a weight by one 1/256 step
+    assert np.abs(lit.rgb.reshape(-1, 3) - ref).max() < 2e-2
+    assert np.median(np.abs(lit.rgb.reshape(-1, 3) - ref)) < 1e-5
