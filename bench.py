@@ -185,7 +185,8 @@ def served_legs(args, rend, local):
     # serving: Poisson arrivals, random orbit cameras, mixed sizes and spp, denoised
     srv = wrk.Server(device=local)
     srv.set_denoiser(dn)
-    out["serving"] = serve_bench.run(srv, scene, n_requests=args.serve_requests, rate=50.0, device=local)
+    out["serving"] = serve_bench.run(srv, scene, n_requests=args.serve_requests, rate=50.0, device=local,
+                                     audit_renderer=rend)
     out["serving"]["scene"] = "scale_test (~2.41M tris), resident"
     del srv
     return out
@@ -341,7 +342,11 @@ def main():
         sd.settings.spp = args.spp
     st = sd.settings
     scene = wrk.Scene.from_data(sd, device=local)
-    rend = wrk.Renderer(device=local)
+    # launch shape (queue capacity, graph chunk, shading block) picked by the
+    # project's autotuner on this workload at 1/16 of its spp
+    tune = wrk.autotune(scene, spp=max(1, st.spp // 16), device=local)
+    rend = wrk.Renderer(device=local, capacity=tune["capacity"])
+    rend.set_launch(tune["chunk"], tune["shadeBlock"])
     npx = st.width * st.height
     frame = torch.zeros(npx * 3, dtype=torch.float32, device=f"cuda:{local}")
     samples_per_step = npx * st.spp
@@ -437,9 +442,11 @@ def main():
             "dtype": "f32",
             "data": "synthetic (seeded procedural scene; no dataset)",
             "config": {"workload": cfg["workload"], "samples_per_step_per_gpu": samples_per_step,
+                       "launch": {k: tune[k] for k in ("capacity", "chunk", "shadeBlock")},
                        "parallelism": f"sample-split x{world}, one NCCL all-reduce of the frame per step"
                        if world > 1 else "single GPU",
-                       "l2": "per-step working set (path slots 4M x 144 B = 604 MB) exceeds the 126 MB L2"},
+                       "l2": f"per-step working set exceeds the 126 MB L2 (path queues: {tune['capacity']} entries "
+                             f"x 928 B = {tune['capacity'] * 928 / 1e9:.1f} GB)"},
             "mrays_per_s": mrays,
             "iterations_per_step": iters / args.steps,
             "gpu_launches": iters * 9 + args.steps * 2,

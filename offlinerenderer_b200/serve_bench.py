@@ -17,8 +17,32 @@ from . import scenes, wrk
 from .denoise_train import orbit_camera
 
 
+def audit(server: "wrk.Server", renderer: "wrk.Renderer", scene: "wrk.Scene", jobs, ref_spp: int = 512,
+          device: int = 0) -> list:
+    """relMSE of served images against FP64-accumulated references: each audited
+    request is served again (same camera, size, spp and seed, so the same samples),
+    its denoised result and the plain render are compared with a ref_spp reference."""
+    import torch
+
+    from . import quality
+
+    out = []
+    for cam, st in jobs:
+        H, W = st.height, st.width
+        ref = quality.reference(renderer, scene, cam, st, total_spp=ref_spp, chunk=128, device=device)
+        served = torch.empty((H, W, 3), dtype=torch.float32, device=f"cuda:{device}")
+        tk = server.submit(scene, camera=cam, settings=st, denoise=True)
+        server.wait(tk)
+        server.result_device(tk, served.data_ptr())
+        plain, _, _, _ = quality.render(renderer, scene, cam, st, st.spp, 0, torch, device, guides=False)
+        out.append({"size": W, "spp": st.spp, "relmse_served": quality.relmse(served, ref),
+                    "relmse_plain": quality.relmse(plain, ref), "reference_spp": ref_spp})
+    return out
+
+
 def run(server: "wrk.Server", scene: "wrk.Scene", n_requests: int = 400, rate: float = 50.0, seed: int = 7,
-        resolutions=(256, 512, 1024), spps=(1, 4, 16), denoise: bool = True, device: int = 0) -> dict:
+        resolutions=(256, 512, 1024), spps=(1, 4, 16), denoise: bool = True, device: int = 0,
+        audit_renderer=None, audit_requests: int = 4) -> dict:
     import torch
 
     rng = np.random.default_rng(seed)
@@ -63,7 +87,17 @@ def run(server: "wrk.Server", scene: "wrk.Scene", n_requests: int = 400, rate: f
             samples += nsamp
     wall = time.perf_counter() - t0
     lat_ms = np.asarray(lat) * 1e3
-    return {"requests": n_requests, "rate_per_s": rate, "resolutions": list(resolutions), "spps": list(spps),
+    checked = []
+    if audit_renderer is not None and audit_requests:
+        pick = np.random.default_rng(seed + 1).choice(n_requests, audit_requests, replace=False)
+        small = [jobs[int(k)] for k in pick]
+        # keep the audit bounded: references of the 1024^2 requests at 256^2 of the same view
+        small = [(c, st) if st.width <= 512 else
+                 (c, scenes.RenderSettings(256, 256, st.spp, maxBounces=st.maxBounces,
+                                           russianRouletteDepth=st.russianRouletteDepth, seed=st.seed))
+                 for c, st in small]
+        checked = audit(server, audit_renderer, scene, small, device=device)
+    return {"audit": checked, "requests": n_requests, "rate_per_s": rate, "resolutions": list(resolutions), "spps": list(spps),
             "denoised": denoise, "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
             "mean_ms": float(lat_ms.mean()), "max_ms": float(lat_ms.max()),
             "mean_wait_ms": float(np.mean(wait) * 1e3), "mean_service_ms": float(np.mean(service) * 1e3),
