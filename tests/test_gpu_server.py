@@ -162,3 +162,33 @@ def test_batched_variant_scenes_each_as_alone(gpu):
         rgb, alb, nrm, _ = srv.result(t)
         solo = _solo(gpu, sc, sc._data.camera, st)
         assert _close(rgb, solo.rgb) and _close(nrm, solo.normal)
+
+
+def test_server_rejects_bad_requests(gpu, world):
+    cb, _ = world
+    srv = gpu.Server(capacity=1 << 13)
+    with pytest.raises(gpu.WrkError):
+        srv.submit(cb, settings=_settings(32, 32, 0, cb._data.settings))  # spp 0
+    with pytest.raises(gpu.WrkError):
+        srv.ready(12345)  # unknown ticket
+    with pytest.raises(gpu.WrkError):
+        srv.submit(cb, settings=_settings(32, 32, 1, cb._data.settings), denoise=True)  # no denoiser attached
+    st = srv.step()  # nothing queued: a no-op
+    assert st["running"] == 0 and st["queued"] == 0
+
+
+def test_sample_split_across_requests(gpu, world):
+    """Two requests over disjoint sample ranges [0, 4) and [4, 8) average to the
+    request over [0, 8): the RNG is keyed by sample index, so they draw the same
+    samples (up to f32 rounding of the sums)."""
+    _, sc = world
+    st4 = _settings(64, 64, 4, sc._data.settings)
+    st8 = _settings(64, 64, 8, sc._data.settings)
+    srv = gpu.Server(capacity=1 << 15)
+    a = srv.submit(sc, settings=st4, sample_offset=0)
+    b = srv.submit(sc, settings=st4, sample_offset=4)
+    c = srv.submit(sc, settings=st8)
+    for t in (a, b, c):
+        srv.wait(t)
+    ra, rb, rc = srv.result(a)[0], srv.result(b)[0], srv.result(c)[0]
+    np.testing.assert_allclose(0.5 * (ra + rb), rc, rtol=2e-5, atol=2e-6)
