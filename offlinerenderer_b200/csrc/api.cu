@@ -163,6 +163,7 @@ namespace wrk {
 Engine::~Engine() {
     if (stream) cudaStreamSynchronize(stream);
     if (graph) cudaGraphExecDestroy(graph);
+    if (loopGraph) cudaGraphExecDestroy(loopGraph);
     for (cudaEvent_t e : stageEv) cudaEventDestroy(e);
     if (hCtr) cudaFreeHost(hCtr);
     if (hCtl) cudaFreeHost(hCtl);
@@ -305,6 +306,64 @@ cudaError_t Engine::enqueue_chunk(const DevScene& s0, bool multi, bool timing) {
         }
         if ((e = cudaGraphLaunch(graph, stream)) != cudaSuccess) return e;
     }
+    if ((e = cudaMemcpyAsync(hCtr, q.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, stream)) != cudaSuccess) return e;
+    return cudaMemcpyAsync(hCtl, dCtl, sizeof(SlotCtl) * kMaxSlots, cudaMemcpyDeviceToHost, stream);
+}
+
+cudaError_t Engine::enqueue_until_done(const DevScene& s0, bool multi, uint32_t iterLimit) {
+    if (loopUnsupported) return cudaErrorNotSupported;
+    cudaError_t e;
+    const bool same = loopGraph && multi == loopMulti && memcmp(&s0, &loopScene, sizeof(DevScene)) == 0 &&
+                      loopCfg.chunk == cfg.chunk && loopCfg.shadeBlock == cfg.shadeBlock &&
+                      loopCfg.traceBlocksPerSM == cfg.traceBlocksPerSM &&
+                      loopCfg.shadeBlocksPerSM == cfg.shadeBlocksPerSM;
+    if (!same) {
+        if (loopGraph) cudaGraphExecDestroy(loopGraph);
+        loopGraph = nullptr;
+        cudaGraph_t g = nullptr;
+        if ((e = cudaGraphCreate(&g, 0)) != cudaSuccess) return e;
+        cudaGraphConditionalHandle h;
+        cudaGraphNodeParams np{};
+        cudaGraphNode_t node;
+        e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess) {
+            np.type = cudaGraphNodeTypeConditional;
+            np.conditional.handle = h;
+            np.conditional.type = cudaGraphCondTypeWhile;
+            np.conditional.size = 1;
+            e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphDestroy(g);
+            loopUnsupported = true;
+            return cudaErrorNotSupported;
+        }
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        if ((e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+            cudaSuccess) {
+            cudaGraphDestroy(g);
+            return e;
+        }
+        for (uint32_t k = 0; k < cfg.chunk; ++k) launch_iteration(*this, s0, multi, stream, nullptr);
+        launch_loop_cond(h, q, stream);
+        cudaGraph_t captured = nullptr;
+        e = cudaStreamEndCapture(stream, &captured);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&loopGraph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            loopGraph = nullptr;
+            return e;
+        }
+        loopMulti = multi;
+        memcpy(&loopScene, &s0, sizeof(DevScene));
+        loopCfg = cfg;
+    }
+    hGenOrder[kMaxSlots + 2] = iterLimit;  // staging word for Counters::iterLimit
+    if ((e = cudaMemcpyAsync(&q.ctr->iterLimit, &hGenOrder[kMaxSlots + 2], sizeof(uint32_t), cudaMemcpyHostToDevice,
+                             stream)) != cudaSuccess)
+        return e;
+    if ((e = cudaGraphLaunch(loopGraph, stream)) != cudaSuccess) return e;
     if ((e = cudaMemcpyAsync(hCtr, q.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, stream)) != cudaSuccess) return e;
     return cudaMemcpyAsync(hCtl, dCtl, sizeof(SlotCtl) * kMaxSlots, cudaMemcpyDeviceToHost, stream);
 }
@@ -692,7 +751,22 @@ static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, con
     float stageMs[WRK_NUM_STAGES] = {0};
     uint32_t stageN[WRK_NUM_STAGES] = {0};
     CK(cudaEventRecord(r->evLoop0, st));
-    while (true) {
+    bool looped = false;
+    if (!timing) {
+        // device-driven: one graph launch runs chunks until the request finished
+        cudaError_t e = E.enqueue_until_done(s->view, false, (uint32_t)std::min<unsigned long long>(maxIters, 0xffffffffu));
+        if (e == cudaSuccess) {
+            CK(cudaStreamSynchronize(st));
+            iters = E.hCtr->iteration;
+            if (E.hCtr->error) return fail(WRK_ERR_DEVICE, "device error flags 0x%x during render", E.hCtr->error);
+            if (!slot_finished(E.hCtl[0]))
+                return fail(WRK_ERR_DEVICE, "render did not converge after %u iterations", iters);
+            looped = true;
+        } else if (e != cudaErrorNotSupported) {
+            return fail(WRK_ERR_CUDA, "device-driven render loop: %s", cudaGetErrorString(e));
+        }
+    }
+    while (!looped) {
         CK(E.enqueue_chunk(s->view, false, timing));
         iters += E.cfg.chunk;
         CK(cudaStreamSynchronize(st));

@@ -65,6 +65,13 @@ struct Engine {
     bool graphMulti = false;
     LaunchConfig graphCfg;
     std::vector<cudaEvent_t> stageEv;
+    // device-driven loop: one graph launch repeats chunks (a conditional WHILE node)
+    // until every request in the admission order finished
+    cudaGraphExec_t loopGraph = nullptr;
+    DevScene loopScene{};
+    bool loopMulti = false;
+    bool loopUnsupported = false;
+    LaunchConfig loopCfg;
 
     ~Engine();
     // Allocates queues (capacity path entries) and tables; returns a cudaError_t.
@@ -74,6 +81,10 @@ struct Engine {
     // Enqueues cfg.chunk iterations (graph, or plain launches with per-stage events
     // when `timing` is set), then the readback of counters and slot progress.
     cudaError_t enqueue_chunk(const DevScene& s0, bool multi, bool timing);
+    // Enqueues the device-driven loop (chunks until done or `iterLimit` iterations),
+    // then the readback.  Returns cudaErrorNotSupported when conditional graph nodes
+    // are unavailable (the caller then steps chunk by chunk from the host).
+    cudaError_t enqueue_until_done(const DevScene& s0, bool multi, uint32_t iterLimit);
     // Adds the per-stage times of the last timed chunk.
     cudaError_t stage_times(float* ms, uint32_t* launches);
     int trace_grid() const { return numSMs * (int)cfg.traceBlocksPerSM; }

@@ -88,7 +88,7 @@ __global__ void k_control(Queues q) {
         if (slot >= kMaxSlots) continue;
         SlotCtl& sc = q.ctl[slot];
         if (sc.state != kSlotActive) continue;
-        if (sc.workNext >= sc.workTotal && sc.finished >= sc.workTotal) {
+        if (slot_finished(sc)) {
             sc.state = kSlotDone;
             sc.doneNs = now;
             sc.doneIter = c->iteration;
@@ -115,6 +115,25 @@ __global__ void k_control(Queues q) {
 }
 
 void launch_control(const Queues& q, cudaStream_t st) { k_control<<<1, 1, 0, st>>>(q); }
+
+// One thread: the conditional graph node repeats its chunk while any request in the
+// admission order is still active and unfinished, no device error was raised and
+// the iteration bound is not reached.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, Queues q) {
+    const Counters* c = q.ctr;
+    const uint32_t n = min(q.genOrder[0], kMaxSlots);
+    bool busy = false;
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t slot = q.genOrder[1 + k];
+        if (slot < kMaxSlots && q.ctl[slot].state == kSlotActive && !slot_finished(q.ctl[slot])) busy = true;
+    }
+    const bool go = busy && c->error == 0 && c->iteration < c->iterLimit;
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+void launch_loop_cond(cudaGraphConditionalHandle h, const Queues& q, cudaStream_t st) {
+    k_loop_cond<<<1, 1, 0, st>>>(h, q);
+}
 
 // Camera ray for (pixel, sample) of the request a work item belongs to: trace.cu:54-125.
 __global__ void __launch_bounds__(kShadeBlock) k_generate(Queues q) {

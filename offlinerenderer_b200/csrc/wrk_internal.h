@@ -121,7 +121,7 @@ struct Counters {
     uint32_t iteration;
     uint32_t error;
     uint32_t activeSlots;  // slots still active after this iteration's completion check
-    uint32_t pad;
+    uint32_t iterLimit;    // the device-driven loop stops after this many iterations
     unsigned long long extRays;
     unsigned long long shdRays;
     unsigned long long paths;
@@ -190,6 +190,12 @@ void launch_trace_shadow(const DevScene& s, const Queues& q, bool multi, int gri
 void launch_shade_bucket(uint32_t bucket, const DevScene& s, const Queues& q, bool multi, int grid, int block,
                          cudaStream_t st);
 void launch_resolve(const Frame& f, uint32_t rawGuides, float* rgb, float* albedo, float* normal, cudaStream_t st);
+// End of one chunk of the device-driven loop: keeps the enclosing conditional
+// WHILE graph node running while a request in the admission order has work left.
+void launch_loop_cond(cudaGraphConditionalHandle h, const Queues& q, cudaStream_t st);
+__host__ __device__ inline bool slot_finished(const SlotCtl& sc) {
+    return sc.workNext >= sc.workTotal && sc.finished >= sc.workTotal;
+}
 
 // BVH build (bvh_build.cu)
 struct BvhBuildResult {
