@@ -212,7 +212,7 @@ def batched_scenes_leg(local):
     srv.wait(srv.submit(scs[0], settings=scenes.RenderSettings(64, 64, 1)))  # graph capture
     out = torch.empty((1024 * 1024 * 3,), dtype=torch.float32, device=f"cuda:{local}")
     for t in list(srv._shapes):
-        srv.result_device(t, out.data_ptr())
+        srv.result_device(t, wrk.TensorPtr(out).ptr)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     pending = [srv.submit(sc) for sc in scs]
@@ -222,7 +222,7 @@ def batched_scenes_leg(local):
         steps += 1
         gpu_ms += st["lastChunkMs"]
         for t in [t for t in pending if srv.ready(t)]:
-            srv.result_device(t, out.data_ptr())
+            srv.result_device(t, wrk.TensorPtr(out).ptr)
             pending.remove(t)
     wall = time.perf_counter() - t1
     samples = sum(sd.settings.width * sd.settings.height * sd.settings.spp for sd in sds)
@@ -353,7 +353,8 @@ def main():
 
     def step(i):
         off = (i * world + rank) * st.spp
-        s = rend.render_device(scene, None, d_rgb_ptr=frame.data_ptr(), sample_offset=off)
+        # TensorPtr waits for torch's stream (the previous step's all-reduce reads the frame)
+        s = rend.render_device(scene, None, d_rgb_ptr=wrk.TensorPtr(frame).ptr, sample_offset=off)
         if dist is not None:
             dist.all_reduce(frame)  # combine the ranks' sample ranges
         return s
@@ -388,7 +389,7 @@ def main():
     mrays = world * rays / (ms / 1e3) / 1e6
 
     # per-stage device times (events on the renderer's stream), one extra render
-    tst = rend.render_device(scene, None, d_rgb_ptr=frame.data_ptr(), stage_timing=True)
+    tst = rend.render_device(scene, None, d_rgb_ptr=wrk.TensorPtr(frame).ptr, stage_timing=True)
     stage_ms = tst["stageMs"]
     units = {"trace_extension": tst["extensionRays"], "trace_shadow": tst["shadowRays"],
              "shade_lambert": tst["bucketPaths"]["lambert"], "shade_dielectric": tst["bucketPaths"]["dielectric"],

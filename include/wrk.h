@@ -320,6 +320,12 @@ int wrk_denoiser_set_params(wrk_denoiser* d, const float* h_params, uint64_t n);
  * parameter gradients (copied to h_grads when not NULL). */
 int wrk_denoiser_gradients(wrk_denoiser* d, const float* d_rgb, const float* d_albedo, const float* d_normal,
                            const float* d_target, uint32_t B, uint32_t H, uint32_t W, float* h_grads, float* loss);
+/* Data-parallel training: copy the last pass's gradients out to device memory
+ * (num_params floats), overwrite them (e.g. with the average across ranks), and
+ * apply one Adam step with the current gradients. */
+int wrk_denoiser_grads_copy(wrk_denoiser* d, float* d_out);
+int wrk_denoiser_grads_set(wrk_denoiser* d, const float* d_in);
+int wrk_denoiser_apply(wrk_denoiser* d, float lr);
 /* The same followed by one Adam step with learning rate lr. */
 int wrk_denoiser_train_step(wrk_denoiser* d, const float* d_rgb, const float* d_albedo, const float* d_normal,
                             const float* d_target, uint32_t B, uint32_t H, uint32_t W, float lr, float* loss);

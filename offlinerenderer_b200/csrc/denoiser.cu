@@ -654,6 +654,18 @@ int fwd_bwd(wrk_denoiser* d, const float* rgb, const float* alb, const float* nr
     return check_err(d, "denoiser forward/backward");
 }
 
+// One Adam step (Kingma & Ba 2015) with the current gradients, then the bf16 re-layout.
+int adam_step(wrk_denoiser* d, float lr) {
+    d->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    float c1 = 1.0f - std::pow(b1, (float)d->step), c2 = 1.0f - std::pow(b2, (float)d->step);
+    k_adam<<<grid_for(d->nparams), 256, 0, d->stream>>>(d->params.as<float>(), d->grads.as<float>(),
+                                                        d->adamM.as<float>(), d->adamV.as<float>(), d->nparams, lr, b1,
+                                                        b2, 1e-8f, c1, c2);
+    DCK(cudaGetLastError());
+    return relayout_all(d);
+}
+
 }  // namespace
 
 extern "C" {
@@ -798,16 +810,38 @@ int wrk_denoiser_train_step(wrk_denoiser* d, const float* rgb, const float* alb,
     DCK(cudaEventRecord(d->ev0, d->stream));
     int rc = fwd_bwd(d, rgb, alb, nrm, target, B, H, W, loss);
     if (rc) return rc;
-    d->step += 1;
-    const float b1 = 0.9f, b2 = 0.999f;
-    float c1 = 1.0f - std::pow(b1, (float)d->step), c2 = 1.0f - std::pow(b2, (float)d->step);
-    k_adam<<<grid_for(d->nparams), 256, 0, d->stream>>>(d->params.as<float>(), d->grads.as<float>(),
-                                                        d->adamM.as<float>(), d->adamV.as<float>(), d->nparams, lr, b1,
-                                                        b2, 1e-8f, c1, c2);
-    if ((rc = relayout_all(d))) return rc;
+    if ((rc = adam_step(d, lr))) return rc;
     DCK(cudaEventRecord(d->ev1, d->stream));
     DCK(cudaStreamSynchronize(d->stream));
     cudaEventElapsedTime(&d->lastMs, d->ev0, d->ev1);
+    return WRK_OK;
+}
+
+// Data-parallel training: the gradients of the last forward / backward pass are
+// copied out (device to device), averaged across ranks by the caller's collective,
+// written back, and applied.
+int wrk_denoiser_grads_copy(wrk_denoiser* d, float* d_out) {
+    if (!d || !d_out) return dfail(WRK_ERR_INVALID, "null argument");
+    DCK(cudaSetDevice(d->device));
+    DCK(cudaMemcpyAsync(d_out, d->grads.p, d->nparams * 4, cudaMemcpyDeviceToDevice, d->stream));
+    DCK(cudaStreamSynchronize(d->stream));
+    return WRK_OK;
+}
+
+int wrk_denoiser_grads_set(wrk_denoiser* d, const float* d_in) {
+    if (!d || !d_in) return dfail(WRK_ERR_INVALID, "null argument");
+    DCK(cudaSetDevice(d->device));
+    DCK(cudaMemcpyAsync(d->grads.p, d_in, d->nparams * 4, cudaMemcpyDeviceToDevice, d->stream));
+    DCK(cudaStreamSynchronize(d->stream));
+    return WRK_OK;
+}
+
+int wrk_denoiser_apply(wrk_denoiser* d, float lr) {
+    if (!d) return dfail(WRK_ERR_INVALID, "null denoiser");
+    DCK(cudaSetDevice(d->device));
+    int rc = adam_step(d, lr);
+    if (rc) return rc;
+    DCK(cudaStreamSynchronize(d->stream));
     return WRK_OK;
 }
 

@@ -22,10 +22,7 @@ UNET_LAYERS = [(16, 32, 0), (32, 32, 0), (32, 64, 1), (64, 64, 1), (64, 128, 2),
 FLOP_PER_PX = sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in UNET_LAYERS)
 
 
-class _Ptr:
-    def __init__(self, t):
-        self.t = t
-        self.ptr = t.data_ptr()
+_Ptr = wrk.TensorPtr
 
 
 def main():

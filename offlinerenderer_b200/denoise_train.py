@@ -1,6 +1,7 @@
 """Training of the learned denoiser, on the GPU end to end.
 
-    python -m offlinerenderer_b200.denoise_train [--scenes 8] [--views 16] [--steps 3000] [--out PATH]
+    python -m offlinerenderer_b200.denoise_train [--scenes 16] [--views 24] [--steps 12000] [--out PATH]
+    python -m torch.distributed.run --nproc-per-node N -m offlinerenderer_b200.denoise_train ...   (data parallel)
 
 The renderer itself generates the training pairs: seeded variants of the
 scale-test scene (heightfield + 250 icospheres of the five BSDFs + 64 emissive
@@ -50,12 +51,7 @@ def orbit_camera(rng, width: int, height: int, center=(0.5, 0.05, 0.5)) -> scene
                          fovY=fov, aspect=float(np.float32(width) / np.float32(height)))
 
 
-class _Ptr:
-    """Device address wrapper accepted wherever the binding takes a DeviceArray."""
-
-    def __init__(self, t):
-        self.t = t
-        self.ptr = t.data_ptr()
+_Ptr = wrk.TensorPtr
 
 
 def render_views(scene, renderer, cams, size, spp, sample_offset, torch, device):
@@ -68,7 +64,7 @@ def render_views(scene, renderer, cams, size, spp, sample_offset, torch, device)
     st = scenes.RenderSettings(size, size, spp, maxBounces=st.maxBounces, russianRouletteDepth=st.russianRouletteDepth,
                                seed=st.seed, useNEE=st.useNEE)
     for v, cam in enumerate(cams):
-        renderer.render_device(scene, None, camera=cam, settings=st, d_rgb_ptr=rgb[v].data_ptr(),
+        renderer.render_device(scene, None, camera=cam, settings=st, d_rgb_ptr=_Ptr(rgb[v]).ptr,
                                d_albedo=_Ptr(alb[v]), d_normal=_Ptr(nrm[v]), sample_offset=sample_offset)
     return rgb, alb, nrm
 
@@ -105,12 +101,28 @@ def generate(scene_seeds, views, size, target_spp, device=0, log=print):
     return data
 
 
-def train(data, steps, batch=16, crop=128, lr=1e-3, seed=1, device=0, log=print, dn=None):
+def dp_step(dn, dist, gbuf, d_rgb, d_alb, d_nrm, d_tgt, B, H, W, lr) -> float:
+    """One data-parallel step: local forward / backward, gradients averaged across
+    ranks with one all-reduce, then the same Adam step on every rank (the weights
+    stay identical because every rank starts from the same seed)."""
+    loss = dn.gradients_device(d_rgb, d_alb, d_nrm, d_tgt, B, H, W)
+    dn.grads_copy(_Ptr(gbuf).ptr)
+    dist.all_reduce(gbuf)
+    gbuf /= dist.get_world_size()
+    dn.grads_set(_Ptr(gbuf).ptr)  # waits for the all-reduce and the division on torch's stream
+    dn.apply(lr)
+    return loss
+
+
+def train(data, steps, batch=16, crop=128, lr=1e-3, seed=1, device=0, log=print, dn=None, dist=None):
     import torch
 
+    rank = dist.get_rank() if dist is not None else 0
+    world = dist.get_world_size() if dist is not None else 1
     g = torch.Generator(device=f"cuda:{device}")
-    g.manual_seed(seed)
+    g.manual_seed(seed + 7919 * rank)  # every rank draws its own crops
     dn = dn or wrk.Denoiser(device=device, seed=seed)
+    gbuf = torch.empty(dn.num_params, dtype=torch.float32, device=f"cuda:{device}") if world > 1 else None
     V, S = data["target"].shape[0], data["target"].shape[1]
     losses = []
     t0 = time.time()
@@ -133,7 +145,10 @@ def train(data, steps, batch=16, crop=128, lr=1e-3, seed=1, device=0, log=print,
             rgb, alb, nrm, tgt = (t.flip(2).contiguous() for t in (rgb, alb, nrm, tgt))
             nrm[..., 0] = -nrm[..., 0]
         cur = lr * (0.1 + 0.9 * 0.5 * (1.0 + math.cos(math.pi * it / max(1, steps))))
-        loss = dn.train_step(_Ptr(rgb), _Ptr(alb), _Ptr(nrm), _Ptr(tgt), batch, crop, crop, cur)
+        if world > 1:
+            loss = dp_step(dn, dist, gbuf, _Ptr(rgb), _Ptr(alb), _Ptr(nrm), _Ptr(tgt), batch, crop, crop, cur)
+        else:
+            loss = dn.train_step(_Ptr(rgb), _Ptr(alb), _Ptr(nrm), _Ptr(tgt), batch, crop, crop, cur)
         losses.append(loss)
         if it % 250 == 0 or it == steps - 1:
             log(f"step {it}: loss {np.mean(losses[-50:]):.4f} lr {cur:.2e} ({time.time() - t0:.1f} s)")
@@ -174,11 +189,11 @@ def load_weights(dn: "wrk.Denoiser", path: str = DEFAULT_WEIGHTS) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--scenes", type=int, default=8)
-    ap.add_argument("--views", type=int, default=16)
+    ap.add_argument("--scenes", type=int, default=16)
+    ap.add_argument("--views", type=int, default=24)
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--target-spp", type=int, default=1024)
-    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--steps", type=int, default=12000)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
@@ -194,18 +209,36 @@ def main():
 
     import torch
 
+    # one process per GPU under torch.distributed.run: every rank renders its own
+    # share of the scene variants and the gradients are averaged each step
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     t0 = time.time()
-    data = generate(list(range(101, 101 + args.scenes)), args.views, args.size, args.target_spp, log=log)
+    seeds = list(range(101, 101 + args.scenes))[rank::world]
+    data = generate(seeds, args.views, args.size, args.target_spp, device=local, log=log)
     gen_s = time.time() - t0
-    dn, losses, train_s = train(data, args.steps, batch=args.batch, lr=args.lr, log=log)
+    dn, losses, train_s = train(data, args.steps, batch=args.batch, lr=args.lr, device=local, log=log, dist=dist)
     meta = {"scenes": list(range(101, 101 + args.scenes)), "views": args.views, "size": args.size,
             "target_spp": args.target_spp, "input_spps": list(INPUT_SPPS), "steps": args.steps, "batch": args.batch,
             "crop": 128, "lr": args.lr, "gen_s": gen_s, "train_s": train_s,
             "final_loss": float(np.mean(losses[-100:]))}
-    save_weights(dn, args.out, meta)
-    log(json.dumps(meta))
+    meta["ranks"] = world
+    if rank == 0:
+        save_weights(dn, args.out, meta)
+        log(json.dumps(meta))
     del data
     torch.cuda.empty_cache()
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

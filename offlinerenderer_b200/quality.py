@@ -15,10 +15,7 @@ import numpy as np
 from . import scenes, wrk
 
 
-class _Ptr:
-    def __init__(self, t):
-        self.t = t
-        self.ptr = t.data_ptr()
+_Ptr = wrk.TensorPtr
 
 
 def relmse(x, ref) -> float:
@@ -57,7 +54,7 @@ def render(renderer, scene, cam, st, spp, sample_offset, torch, device=0, guides
     rgb = torch.empty((H, W, 3), dtype=torch.float32, device=f"cuda:{device}")
     alb = torch.empty_like(rgb) if guides else None
     nrm = torch.empty_like(rgb) if guides else None
-    s = renderer.render_device(scene, None, camera=cam, settings=_settings(st, spp), d_rgb_ptr=rgb.data_ptr(),
+    s = renderer.render_device(scene, None, camera=cam, settings=_settings(st, spp), d_rgb_ptr=_Ptr(rgb).ptr,
                                d_albedo=_Ptr(alb) if guides else None, d_normal=_Ptr(nrm) if guides else None,
                                sample_offset=sample_offset)
     return rgb, alb, nrm, s["gpuMs"]

@@ -33,7 +33,7 @@ def audit(server: "wrk.Server", renderer: "wrk.Renderer", scene: "wrk.Scene", jo
         served = torch.empty((H, W, 3), dtype=torch.float32, device=f"cuda:{device}")
         tk = server.submit(scene, camera=cam, settings=st, denoise=True)
         server.wait(tk)
-        server.result_device(tk, served.data_ptr())
+        server.result_device(tk, wrk.TensorPtr(served).ptr)
         plain, _, _, _ = quality.render(renderer, scene, cam, st, st.spp, 0, torch, device, guides=False)
         out.append({"size": W, "spp": st.spp, "relmse_served": quality.relmse(served, ref),
                     "relmse_plain": quality.relmse(plain, ref), "reference_spp": ref_spp})
@@ -79,7 +79,7 @@ def run(server: "wrk.Server", scene: "wrk.Scene", n_requests: int = 400, rate: f
         busy_ms += s["lastChunkMs"]
         for tk in [t for t in pending if server.ready(t)]:
             arr, t_sub, nsamp = pending.pop(tk)
-            info = server.result_device(tk, out.data_ptr())
+            info = server.result_device(tk, wrk.TensorPtr(out).ptr)
             ready = t_sub + (info["readyMs"] - info["submitMs"]) / 1e3
             lat.append(ready - arr)
             wait.append((t_sub - arr) + (info["admitMs"] - info["submitMs"]) / 1e3)

@@ -154,6 +154,9 @@ SIGNATURES = {
     "wrk_denoiser_train_step": ([_VP, _VP, _VP, _VP, _VP, _U32, _U32, _U32, _F, C.POINTER(_F)], _I),
     "wrk_denoiser_infer": ([_VP, _VP, _VP, _VP, _U32, _U32, _U32, _VP], _I),
     "wrk_denoiser_last_ms": ([_VP, C.POINTER(_F)], _I),
+    "wrk_denoiser_grads_copy": ([_VP, _VP], _I),
+    "wrk_denoiser_grads_set": ([_VP, _VP], _I),
+    "wrk_denoiser_apply": ([_VP, _F], _I),
     "wrk_denoiser_load": ([_VP, C.c_char_p], _I),
 }
 
@@ -216,6 +219,20 @@ class DeviceArray:
         if p and _lib is not None:
             _lib.wrk_free(p)
             self.ptr = None
+
+
+class TensorPtr:
+    """A torch CUDA tensor passed where the binding takes a DeviceArray.  The library
+    works on its own CUDA streams, so the work torch queued to produce the tensor is
+    waited for here, before the library reads it."""
+
+    def __init__(self, t):
+        import torch
+
+        if t.is_cuda:
+            torch.cuda.current_stream(t.device).synchronize()
+        self.t = t
+        self.ptr = t.data_ptr()
 
 
 def camera_struct(cam) -> CameraC:
@@ -589,6 +606,22 @@ class Denoiser:
         _check(lib().wrk_denoiser_gradients(self.handle, d_rgb.ptr, self._ptr(d_alb), self._ptr(d_nrm), d_target.ptr,
                                             B, H, W, g.ctypes.data, C.byref(loss)))
         return loss.value, g
+
+    def gradients_device(self, d_rgb, d_alb, d_nrm, d_target, B, H, W) -> float:
+        """Forward + backward; the gradients stay on the device (grads_copy reads them)."""
+        loss = C.c_float()
+        _check(lib().wrk_denoiser_gradients(self.handle, d_rgb.ptr, self._ptr(d_alb), self._ptr(d_nrm),
+                                            d_target.ptr, B, H, W, None, C.byref(loss)))
+        return loss.value
+
+    def grads_copy(self, d_out_ptr: int) -> None:
+        _check(lib().wrk_denoiser_grads_copy(self.handle, d_out_ptr))
+
+    def grads_set(self, d_in_ptr: int) -> None:
+        _check(lib().wrk_denoiser_grads_set(self.handle, d_in_ptr))
+
+    def apply(self, lr: float) -> None:
+        _check(lib().wrk_denoiser_apply(self.handle, lr))
 
     def train_step(self, d_rgb, d_alb, d_nrm, d_target, B, H, W, lr: float) -> float:
         loss = C.c_float()
