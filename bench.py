@@ -447,7 +447,7 @@ def main():
                        "parallelism": f"sample-split x{world}, one NCCL all-reduce of the frame per step"
                        if world > 1 else "single GPU",
                        "l2": f"per-step working set exceeds the 126 MB L2 (path queues: {tune['capacity']} entries "
-                             f"x 928 B = {tune['capacity'] * 928 / 1e9:.1f} GB)"},
+                             f"x 832 B = {tune['capacity'] * 832 / 1e9:.1f} GB)"},
             "mrays_per_s": mrays,
             "iterations_per_step": iters / args.steps,
             "gpu_launches": iters * 9 + args.steps * 2,

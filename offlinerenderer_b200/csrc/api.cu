@@ -187,9 +187,11 @@ cudaError_t Engine::init(int dev, uint32_t cap) {
         return e;
     memset(hCtl, 0, sizeof(SlotCtl) * kMaxSlots);
     memset(hGenOrder, 0, sizeof(uint32_t) * (kMaxSlots + 4));
-    // SoA path queues: extension x2 (5 fields), shadow x2 (9 fields), buckets (6 fields)
+    // SoA path queues: extension x2 (5 fields), shadow x2 (9 fields), the four
+    // material buckets the extension trace fills (6 fields); the Lambert-resume
+    // bucket is the shadow queue itself and has no arrays of its own
     size_t C = capacity;
-    const size_t fields = 2 * 5 + 2 * 9 + kNumBuckets * 6;
+    const size_t fields = 2 * 5 + 2 * 9 + kBucketLambertResume * 6;
     if ((e = queues.alloc(C * fields * sizeof(float4))) != cudaSuccess) return e;
     float4* next = queues.as<float4>();
     auto take = [&]() {
@@ -217,7 +219,8 @@ cudaError_t Engine::init(int dev, uint32_t cap) {
         h.sh_d = take();
         h.sh_c = take();
     }
-    for (int b = 0; b < kNumBuckets; ++b) {
+    q.bucket[kBucketLambertResume] = PathQ{};
+    for (int b = 0; b < (int)kBucketLambertResume; ++b) {
         PathQ& x = q.bucket[b];
         x = PathQ{};
         x.ray_o = take();

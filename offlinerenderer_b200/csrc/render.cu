@@ -544,7 +544,9 @@ __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k
     Counters* c = q.ctr;
     const uint32_t cur = c->cur, nxt = cur ^ 1u;
     const uint32_t n = min(c->bucket[kBucket].v, q.capacity);
-    const PathQ in = q.bucket[kBucket];
+    // Lambert paths resuming after their shadow ray are read from the shadow queue,
+    // where the shadow kernel left them (radiance updated in place).
+    const PathQ in = kBucket == kBucketLambertResume ? (cur ? q.shd[1] : q.shd[0]) : q.bucket[kBucket];
     const PathQ ext = nxt ? q.ext[1] : q.ext[0];
     const PathQ shd = nxt ? q.shd[1] : q.shd[0];
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {

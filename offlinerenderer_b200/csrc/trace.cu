@@ -4,9 +4,10 @@
 // there are no RT cores on B200, so traversal is SIMT integer/FP32 work.
 //
 // Per node: five 16-byte loads (__ldg, read-only path), eight quantized slab tests
-// decoded with one FMA per plane.  Internal-child hits go into an 8-bit mask
-// permuted by the ray octant so the lowest set bit is the child nearest the ray's
-// entry corner; leaf-child hits set bits of a triangle mask.  Pending node groups
+// decoded with one byte permute and one directed-rounding FMA per plane.
+// Internal-child hits go into an 8-bit mask permuted by the ray octant so the
+// lowest set bit is the child nearest the ray's entry corner; leaf-child hits set
+// bits of a triangle mask.  Pending node groups
 // (child base + remaining hit bits + internal mask) go on a short stack held in
 // shared memory, spilling to a bounded local array; overflow raises an error bit
 // and ends the ray instead of corrupting memory.
@@ -50,10 +51,12 @@ __device__ __forceinline__ bool mt_rn(const Ray& r, float4 a, float4 b, float4 c
 
 __device__ __forceinline__ uint32_t byte_of(uint32_t w, int k) { return (w >> (8 * k)) & 0xffu; }
 
-// Byte k of w as a float without an int->float conversion: one byte permute
-// builds the bits 0x4B0000bb = 2^23 + b exactly, and 2^23 is subtracted.
-__device__ __forceinline__ float qbyte(uint32_t w, uint32_t k) {
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + k)) - 8388608.0f;
+// Byte k of w as the float 2^15 + b, exactly, without an int->float conversion:
+// one byte permute builds the bits 0x4700bb00 (exponent 2^15, b in mantissa bits
+// 8-15).  The 2^15 bias is folded into the per-node plane offset (see
+// intersect_node), so a plane costs one permute and one FMA.
+__device__ __forceinline__ float qbias(uint32_t w, uint32_t k) {
+    return __uint_as_float(__byte_perm(w, 0x47000000u, 0x7504u | (k << 4)));
 }
 
 // Intersects the 8 children of a node; returns internal hits (permuted by octant)
@@ -69,6 +72,13 @@ __device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, 
     float sy = __uint_as_float(((n0.w >> 8) & 0xffu) << 23) * iy;
     float sz = __uint_as_float(((n0.w >> 16) & 0xffu) << 23) * iz;
     float ax = (px - r.ox) * ix, ay = (py - r.oy) * iy, az = (pz - r.oz) * iz;
+    // plane t = q*s + a = (2^15 + q)*s + (a - 2^15*s).  The biased offsets are
+    // rounded down for near planes and up for far planes, and the plane FMAs round
+    // the same way, so the slab only grows (by at most ~1/256 of a quantization
+    // step): a child box the ray crosses is never rejected.
+    const float axl = __fmaf_rd(-32768.0f, sx, ax), axh = __fmaf_ru(-32768.0f, sx, ax);
+    const float ayl = __fmaf_rd(-32768.0f, sy, ay), ayh = __fmaf_ru(-32768.0f, sy, ay);
+    const float azl = __fmaf_rd(-32768.0f, sz, az), azh = __fmaf_ru(-32768.0f, sz, az);
     imask = n0.w >> 24;
     childBase = n1.x;
     triBase = n1.y;
@@ -88,12 +98,12 @@ __device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, 
         uint32_t xn = s < 4 ? xn0 : xn1, xf = s < 4 ? xf0 : xf1;
         uint32_t yn = s < 4 ? yn0 : yn1, yf = s < 4 ? yf0 : yf1;
         uint32_t zn = s < 4 ? zn0 : zn1, zf = s < 4 ? zf0 : zf1;
-        float t0x = fmaf(qbyte(xn, k), sx, ax);
-        float t1x = fmaf(qbyte(xf, k), sx, ax);
-        float t0y = fmaf(qbyte(yn, k), sy, ay);
-        float t1y = fmaf(qbyte(yf, k), sy, ay);
-        float t0z = fmaf(qbyte(zn, k), sz, az);
-        float t1z = fmaf(qbyte(zf, k), sz, az);
+        float t0x = __fmaf_rd(qbias(xn, k), sx, axl);
+        float t1x = __fmaf_ru(qbias(xf, k), sx, axh);
+        float t0y = __fmaf_rd(qbias(yn, k), sy, ayl);
+        float t1y = __fmaf_ru(qbias(yf, k), sy, ayh);
+        float t0z = __fmaf_rd(qbias(zn, k), sz, azl);
+        float t1z = __fmaf_ru(qbias(zf, k), sz, azh);
         float tn = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, r.tmin));
         float tf = fminf(fminf(t1x, t1y), fminf(t1z, tfar_lim));
         if (tn <= tf * 1.00000024f) {
@@ -355,6 +365,8 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
     const PathQ in = kAnyHit ? q.shd[cur] : q.ext[cur];
     uint32_t* fetch = kAnyHit ? &c->fetchShadow.v : &c->fetchExtension.v;
     const uint32_t lane = threadIdx.x & 31u;
+    // every shadow entry resumes shading in place: the resume bucket is this queue
+    if (kAnyHit && blockIdx.x == 0 && threadIdx.x == 0) c->bucket[kBucketLambertResume].v = n;
     Trav t;
     TraceGeom geo{s0.nodes, s0.tris, s0.numNodes, s0.numTris};
     uint32_t sceneIdx = 0;
@@ -393,21 +405,12 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
         const bool done = active && fin;
         if (kAnyHit) {
             // Shadow stage of __raygen__trace (trace.cu:27-51): add the NEE
-            // contribution if nothing lies in [tmin, tmax], then resume shading.
-            const PathQ& o = q.bucket[kBucketLambertResume];
-            uint32_t pos = warp_append_pos(&c->bucket[kBucketLambertResume].v, done, q.capacity, &c->error);
-            if (done && pos != kInvalidSlot) {
-                float4 rd = in.rad[idx];
-                if (t.pBest == kNoHit) {
-                    float4 cc = in.sh_c[idx];
-                    rd = make_float4(rd.x + cc.x, rd.y + cc.y, rd.z + cc.z, rd.w);
-                }
-                o.ray_o[pos] = in.ray_o[idx];
-                o.ray_d[pos] = in.ray_d[idx];
-                o.hit[pos] = in.hit[idx];
-                o.thr[pos] = in.thr[idx];
-                o.rad[pos] = rd;
-                o.st[pos] = in.st[idx];
+            // contribution to the entry's radiance in place if nothing lies in
+            // [tmin, tmax].  The resume shade reads this queue as it stands, so the
+            // path state is not copied.
+            if (done && t.pBest == kNoHit) {
+                const float4 rd = in.rad[idx], cc = in.sh_c[idx];
+                in.rad[idx] = make_float4(rd.x + cc.x, rd.y + cc.y, rd.z + cc.z, rd.w);
             }
         } else {
             uint32_t bucket = kNumBuckets;

@@ -15,8 +15,9 @@
 //      thr (throughput, prevPdf)   rad (radiance, pixel)   st (seed, rngDim, depth|iter<<16, flags)
 //      sh_o / sh_d (shadow ray)    sh_c (NEE contribution)
 //   Queues: extension (ray_o ray_d thr rad st) and shadow (all nine fields), each
-//   double-buffered across iterations, and five material buckets (ray_o ray_d hit
-//   thr rad st).  No slot indirection and no free list: a path occupies exactly one
+//   double-buffered across iterations, and four material buckets (ray_o ray_d hit
+//   thr rad st); Lambert paths resume from the shadow queue, whose radiance the
+//   shadow kernel updates in place.  No slot indirection and no free list: a path occupies exactly one
 //   entry between iterations, so the room for new camera paths is the capacity
 //   minus the extension and shadow entries the last iteration produced.
 #pragma once
