@@ -49,8 +49,6 @@ __device__ __forceinline__ bool mt_rn(const Ray& r, float4 a, float4 b, float4 c
     return true;
 }
 
-__device__ __forceinline__ uint32_t byte_of(uint32_t w, int k) { return (w >> (8 * k)) & 0xffu; }
-
 // Byte k of w as the float 2^15 + b, exactly, without an int->float conversion:
 // one byte permute builds the bits 0x4700bb00 (exponent 2^15, b in mantissa bits
 // 8-15).  The 2^15 bias is folded into the per-node plane offset (see
@@ -92,6 +90,7 @@ __device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, 
     uint32_t zn0 = iz >= 0.0f ? n3.x : n4.z, zn1 = iz >= 0.0f ? n3.y : n4.w;
     uint32_t zf0 = iz >= 0.0f ? n4.z : n3.x, zf1 = iz >= 0.0f ? n4.w : n3.y;
     const float tfar_lim = tfar_max * 1.00000024f;
+    uint32_t hm = 0;  // children whose slab the ray crosses, by slot
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
         const uint32_t k = s & 3;
@@ -104,17 +103,31 @@ __device__ __forceinline__ void intersect_node(const uint4* __restrict__ nodes, 
         float t1y = __fmaf_ru(qbias(yf, k), sy, ayh);
         float t0z = __fmaf_rd(qbias(zn, k), sz, azl);
         float t1z = __fmaf_ru(qbias(zf, k), sz, azh);
-        float tn = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, r.tmin));
-        float tf = fminf(fminf(t1x, t1y), fminf(t1z, tfar_lim));
-        if (tn <= tf * 1.00000024f) {
-            uint32_t meta = byte_of(s < 4 ? n1.z : n1.w, k);
-            if ((imask >> s) & 1u) {
-                hits |= 1u << (s ^ oct_inv);
-            } else {
-                uint32_t cnt = (meta >> 5) + 1u, off = meta & 31u;
-                tmask |= ((1u << cnt) - 1u) << off;
-            }
-        }
+        // Three-input integer max / min on the float bit patterns.  Non-negative
+        // floats order like their bit patterns; negative ones order reversed, which
+        // only moves tn down and tf up (a larger slab, never a smaller one), and a
+        // negative tf still fails against tn >= tmin >= 0.  No plane distance is
+        // NaN: the inverse directions are finite (trav_init).
+        float tn = __int_as_float(__vimax3_s32(__float_as_int(t0x), __float_as_int(t0y),
+                                               max(__float_as_int(t0z), __float_as_int(r.tmin))));
+        float tf = __int_as_float(__vimin3_s32(__float_as_int(t1x), __float_as_int(t1y),
+                                               min(__float_as_int(t1z), __float_as_int(tfar_lim))));
+        hm |= (tn <= tf * 1.00000024f) ? (1u << s) : 0u;
+    }
+    // internal hits, moved from slot s to bit s ^ oct_inv by three conditional swaps
+    uint32_t ih = hm & imask;
+    if (oct_inv & 1u) ih = ((ih & 0x55u) << 1) | ((ih >> 1) & 0x55u);
+    if (oct_inv & 2u) ih = ((ih & 0x33u) << 2) | ((ih >> 2) & 0x33u);
+    if (oct_inv & 4u) ih = ((ih & 0x0Fu) << 4) | ((ih >> 4) & 0x0Fu);
+    hits = ih;
+    // leaf hits: each adds its run of cnt triangles starting at bit off
+    uint32_t lh = hm & ~imask;
+    while (lh) {
+        const uint32_t j = __ffs(lh) - 1;
+        lh &= lh - 1;
+        const uint32_t meta = ((j < 4 ? n1.z : n1.w) >> (8 * (j & 3u))) & 0xffu;
+        const uint32_t cnt = (meta >> 5) + 1u, off = meta & 31u;
+        tmask |= ((1u << cnt) - 1u) << off;
     }
 }
 
@@ -139,9 +152,13 @@ struct Trav {
 
 __device__ __forceinline__ void trav_init(Trav& t, const Ray& r) {
     t.r = r;
-    t.ix = 1.0f / r.dx;
-    t.iy = 1.0f / r.dy;
-    t.iz = 1.0f / r.dz;
+    // Direction components below 2^-80 in magnitude are replaced by +-2^-80 for
+    // the slab tests only (the triangle test uses the true direction), so inverse
+    // directions and plane distances stay finite and never NaN.
+    const float ooeps = 8.27180613e-25f;
+    t.ix = 1.0f / (fabsf(r.dx) < ooeps ? copysignf(ooeps, r.dx) : r.dx);
+    t.iy = 1.0f / (fabsf(r.dy) < ooeps ? copysignf(ooeps, r.dy) : r.dy);
+    t.iz = 1.0f / (fabsf(r.dz) < ooeps ? copysignf(ooeps, r.dz) : r.dz);
     uint32_t oct = (r.dx < 0.0f ? 1u : 0u) | (r.dy < 0.0f ? 2u : 0u) | (r.dz < 0.0f ? 4u : 0u);
     t.octInv = oct ^ 7u;  // slot of the child nearest the entry corner -> bit 0
     // the root is a one-child node group
