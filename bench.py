@@ -60,8 +60,9 @@ UNET_FLOP_PER_PX = sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in UNET_LAYERS)
 # Algorithmic HBM bytes per unit of work of each loop stage (per path, per ray):
 #   trace_extension: read the ray (origin|tmin, direction|tmax = 32 B) + write the
 #                    hit record (t, prim, material = 16 B)                      = 48 B / ray
-#   trace_shadow:    shadow ray 32 B + contribution 16 B read, radiance 16 B read
-#                    and written, 4 B queue entry (rounded as 100 B / shadow ray)
+#   trace_shadow:    shadow ray 32 B + contribution 16 B + radiance 16 B + state
+#                    16 B read; the continuing path's ray and throughput (48 B) read
+#                    and its extension entry (80 B) written               = 208 B / shadow ray
 #   shade_*:         read direction 16 + hit 16 + path state 48, write state 48 +
 #                    next ray 32                                                = 160 B / path
 # Measured DRAM traffic of the extension-ray traversal kernel per ray: ncu
@@ -70,8 +71,8 @@ UNET_FLOP_PER_PX = sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in UNET_LAYERS)
 # rays (profiles/k_trace_persistent_dram_showcase_16spp.md); traffic per launch of
 # the full workload = this x rays per launch (traffic grows with the rays traced).
 TRACE_EXT_TRAFFIC_BYTES_PER_RAY = 148.4
-STAGE_BYTES = {"trace_extension": 48, "trace_shadow": 100, "shade_lambert": 160, "shade_dielectric": 160,
-               "shade_ggx": 160, "shade_emissive": 160, "shade_lambert_resume": 160}
+STAGE_BYTES = {"trace_extension": 48, "trace_shadow": 208, "shade_lambert": 160, "shade_dielectric": 160,
+               "shade_ggx": 160, "shade_emissive": 160}
 
 
 class ClockSampler:
@@ -393,8 +394,7 @@ def main():
     stage_ms = tst["stageMs"]
     units = {"trace_extension": tst["extensionRays"], "trace_shadow": tst["shadowRays"],
              "shade_lambert": tst["bucketPaths"]["lambert"], "shade_dielectric": tst["bucketPaths"]["dielectric"],
-             "shade_ggx": tst["bucketPaths"]["ggx"], "shade_emissive": tst["bucketPaths"]["other"],
-             "shade_lambert_resume": tst["bucketPaths"]["lambert_resume"]}
+             "shade_ggx": tst["bucketPaths"]["ggx"], "shade_emissive": tst["bucketPaths"]["other"]}
     dominant = max(STAGE_BYTES, key=lambda k: stage_ms[k])
     peak, peak_kind = hbm_peak()
     launches = max(1, tst["stageLaunches"][dominant])

@@ -87,7 +87,7 @@ enum {
     WRK_STAGE_SHADE_DIELECTRIC = 5,
     WRK_STAGE_SHADE_GGX = 6,
     WRK_STAGE_SHADE_EMISSIVE = 7,
-    WRK_STAGE_SHADE_LAMBERT_RESUME = 8,
+    WRK_STAGE_SHADE_LAMBERT_RESUME = 8, /* kept for layout; always 0: the shadow stage continues these paths */
     WRK_NUM_STAGES = 9
 };
 
@@ -101,7 +101,8 @@ typedef struct {
     float totalMs;           /* device time including uploads / readback */
     float stageMs[9];        /* per-stage device time (WRK_FLAG_STAGE_TIMING), indexed by WRK_STAGE_* */
     uint32_t stageLaunches[9];
-    uint64_t bucketPaths[5]; /* paths shaded per bucket: Lambert, dielectric, GGX, emissive/other, Lambert resume */
+    uint64_t bucketPaths[5]; /* paths shaded per bucket: Lambert, dielectric, GGX, emissive/other, and the
+                                Lambert paths the shadow stage continued after their shadow ray */
 } wrk_render_stats;
 
 typedef struct {

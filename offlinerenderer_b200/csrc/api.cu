@@ -187,11 +187,10 @@ cudaError_t Engine::init(int dev, uint32_t cap) {
         return e;
     memset(hCtl, 0, sizeof(SlotCtl) * kMaxSlots);
     memset(hGenOrder, 0, sizeof(uint32_t) * (kMaxSlots + 4));
-    // SoA path queues: extension x2 (5 fields), shadow x2 (9 fields), the four
-    // material buckets the extension trace fills (6 fields); the Lambert-resume
-    // bucket is the shadow queue itself and has no arrays of its own
+    // SoA path queues: extension x2 (5 fields), shadow x2 (8 fields), the four
+    // material buckets the extension trace fills (6 fields)
     size_t C = capacity;
-    const size_t fields = 2 * 5 + 2 * 9 + kBucketLambertResume * 6;
+    const size_t fields = 2 * 5 + 2 * 8 + kBucketLambertResume * 6;
     if ((e = queues.alloc(C * fields * sizeof(float4))) != cudaSuccess) return e;
     float4* next = queues.as<float4>();
     auto take = [&]() {
@@ -211,7 +210,6 @@ cudaError_t Engine::init(int dev, uint32_t cap) {
         h = PathQ{};
         h.ray_o = take();
         h.ray_d = take();
-        h.hit = take();
         h.thr = take();
         h.rad = take();
         h.st = reinterpret_cast<uint4*>(take());
@@ -271,8 +269,10 @@ static void launch_iteration(const Engine& E, const DevScene& s0, bool multi, cu
     if (ev) cudaEventRecord(ev[3], st);
     launch_trace_shadow(s0, E.q, multi, E.trace_grid(), st);
     if (ev) cudaEventRecord(ev[4], st);
+    // four shade kernels; the fifth stage slot (Lambert resume) stays empty: the
+    // shadow kernel continues those paths
     for (uint32_t b = 0; b < kNumBuckets; ++b) {
-        launch_shade_bucket(b, s0, E.q, multi, E.shade_grid(), (int)E.cfg.shadeBlock, st);
+        if (b != kBucketLambertResume) launch_shade_bucket(b, s0, E.q, multi, E.shade_grid(), (int)E.cfg.shadeBlock, st);
         if (ev) cudaEventRecord(ev[5 + b], st);
     }
 }
@@ -378,7 +378,7 @@ cudaError_t Engine::stage_times(float* ms, uint32_t* launches) {
             cudaError_t e = cudaEventElapsedTime(&t, stageEv[k * 10 + j], stageEv[k * 10 + j + 1]);
             if (e != cudaSuccess) return e;
             ms[j] += t;
-            launches[j] += 1;
+            launches[j] += j == WRK_STAGE_SHADE_LAMBERT_RESUME ? 0u : 1u;
         }
     return cudaSuccess;
 }

@@ -14,8 +14,9 @@
 //   generate              camera rays for the next (sample, pixel) work items,
 //                         appended to the extension queue
 //   trace_extension       closest hit -> material bucket, or miss -> accumulate
-//   trace_shadow          any hit for pending NEE rays -> Lambert resume bucket
-//   shade<bucket> x5      closest-hit attributes, guides, emission, BSDF, RR;
+//   trace_shadow          any hit for pending NEE rays; adds the contribution if
+//                         unoccluded, then continues / accumulates / drops the path
+//   shade<bucket> x4      closest-hit attributes, guides, emission, BSDF, RR;
 //                         appends to the next extension / shadow queue
 // A path carries its own iteration count; after `maxIter` iterations (8 = the
 // reference host loop's cap) a live path is dropped unaccumulated, as libWR does.
@@ -351,12 +352,13 @@ __device__ __forceinline__ bool sample_light(const DevScene& s, PathRegs& r, con
     return true;
 }
 
-// A Lambert hit that sends a shadow ray: the shadow ray and contribution, plus the
-// entry (ray and hit record) the path resumes from after the visibility test.
+// A Lambert hit that sends a shadow ray: the shadow ray, its contribution, and what
+// the path does after the visibility test (kCont*; the path's next ray is in the
+// path registers when it continues).
 struct ShadowOut {
     float3 o, d, c;
     float dist;
-    float4 o4, d4, h4;
+    uint32_t cont;
 };
 
 // Shades entry i of a bucket; the path's next state is left in r (and so for a
@@ -419,7 +421,8 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uin
     if (kBucket == kBucketLambert) {
         // getMaterialAlbedo is a pure function of (material, uv): fetch it once
         const float3 al = albedo_of(s, m, h.u, h.v);
-        if (f.useNEE && s.numEmissive > 0 && !(r.flags & kFlagNeeDone)) {
+        bool shadow = false;
+        if (f.useNEE && s.numEmissive > 0) {
             LightSample ls;
             if (sample_light(s, r, h, ls)) {
                 float bpdf = cosine_pdf(ls.cosTheta);
@@ -432,28 +435,50 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uin
                     so.d = ls.toLight;
                     so.dist = ls.dist;
                     so.c = con;
-                    so.o4 = o4;
-                    so.d4 = d4;
-                    so.h4 = h4;
-                    r.flags |= kFlagNeeDone;
-                    out = kOutShadow;
+                    shadow = true;
                 }
             }
         }
-        if (out == kOutNone) {
-            r.flags &= ~kFlagNeeDone;
-            float3 tg, bt;
-            frame(h.n, tg, bt);
-            float u1 = rnd_dim(r.seed, r.dim++);
-            float u2 = rnd_dim(r.seed, r.dim++);
-            float pdf;
-            float3 loc = cosine_hemisphere(u1, u2, pdf);
-            float3 wd = to_world(loc, h.n, tg, bt);
-            r.thr = mul(r.thr, al);
-            r.prevPdf = pdf;
-            r.flags &= ~kFlagPrevDelta;
+        // cosine bounce (lambertian.cuh:65-147): its draws follow the light
+        // sample's three whether or not a shadow ray is sent
+        float3 tg, bt;
+        frame(h.n, tg, bt);
+        float u1 = rnd_dim(r.seed, r.dim++);
+        float u2 = rnd_dim(r.seed, r.dim++);
+        float pdf;
+        float3 loc = cosine_hemisphere(u1, u2, pdf);
+        float3 wd = to_world(loc, h.n, tg, bt);
+        r.thr = mul(r.thr, al);
+        r.prevPdf = pdf;
+        r.flags &= ~kFlagPrevDelta;
+        if (!shadow) {
             if (!rr(f, r, false)) return kOutDone;
             out = next_bounce(f, r, h, wd);
+        } else {
+            // The shadow ray is traced in the next iteration and the path goes on
+            // after it (the reference resumes shading there).  Nothing below
+            // depends on its outcome, so roulette, depth and the iteration bound
+            // are applied now and the shadow kernel carries them out, adding the
+            // contribution first if the light is visible.
+            if (r.iter + 1u >= f.maxIter) return kOutDone;  // dropped with its shadow ray
+            r.iter += 1u;
+            float3 nt;
+            const float xi = rnd_dim(r.seed, r.dim++);
+            if (!russian_roulette(r.thr, r.depth, f.rrStart, xi, nt, false)) {
+                so.cont = kContAccumulate;
+            } else {
+                r.thr = nt;
+                r.d = wd;
+                r.o = offset_origin(h.pos, h.n, wd);
+                r.depth += 1;
+                if (r.depth >= f.maxBounces) so.cont = kContAccumulate;
+                else if (r.iter + 1u >= f.maxIter) so.cont = kContDrop;
+                else {
+                    r.iter += 1u;
+                    so.cont = kContExt;
+                }
+            }
+            return kOutShadow;
         }
     } else if (kBucket == kBucketDielectric) {
         float3 wo = neg(r.d);
@@ -544,14 +569,11 @@ __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k
     Counters* c = q.ctr;
     const uint32_t cur = c->cur, nxt = cur ^ 1u;
     const uint32_t n = min(c->bucket[kBucket].v, q.capacity);
-    // Lambert paths resuming after their shadow ray are read from the shadow queue,
-    // where the shadow kernel left them (radiance updated in place).
-    const PathQ in = kBucket == kBucketLambertResume ? (cur ? q.shd[1] : q.shd[0]) : q.bucket[kBucket];
+    const PathQ in = q.bucket[kBucket];
     const PathQ ext = nxt ? q.ext[1] : q.ext[0];
     const PathQ shd = nxt ? q.shd[1] : q.shd[0];
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const uint32_t i = base + threadIdx.x;
-        constexpr uint32_t kCode = kBucket == kBucketLambertResume ? kBucketLambert : kBucket;
         PathRegs r;
         ShadowOut so;
         int out = kOutNone;
@@ -562,9 +584,9 @@ __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k
             slot = slot_of(st.w);
             const Frame& f = q.req[slot];
             if constexpr (kMulti) {
-                out = shade_one<kCode>(q.scenes[f.scene], in, i, f, r, so, o4, d4, h4, t4, r4, st);
+                out = shade_one<kBucket>(q.scenes[f.scene], in, i, f, r, so, o4, d4, h4, t4, r4, st);
             } else {
-                out = shade_one<kCode>(s0, in, i, f, r, so, o4, d4, h4, t4, r4, st);
+                out = shade_one<kBucket>(s0, in, i, f, r, so, o4, d4, h4, t4, r4, st);
             }
         }
         count_ended(q.ctl, out == kOutDone, slot);
@@ -577,15 +599,16 @@ __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k
             ext.rad[pe] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
             ext.st[pe] = make_uint4(r.seed, r.dim, (r.depth & 0xffffu) | (r.iter << 16), r.flags);
         } else if (ps != kInvalidSlot) {
-            shd.ray_o[ps] = so.o4;
-            shd.ray_d[ps] = so.d4;
-            shd.hit[ps] = so.h4;
-            shd.thr[ps] = make_float4(r.thr.x, r.thr.y, r.thr.z, r.prevPdf);
+            if (so.cont == kContExt) {  // the extension ray the path continues with
+                shd.ray_o[ps] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
+                shd.ray_d[ps] = make_float4(r.d.x, r.d.y, r.d.z, 1e20f);
+                shd.thr[ps] = make_float4(r.thr.x, r.thr.y, r.thr.z, r.prevPdf);
+            }
             shd.rad[ps] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
             shd.st[ps] = make_uint4(r.seed, r.dim, (r.depth & 0xffffu) | (r.iter << 16), r.flags);
             shd.sh_o[ps] = make_float4(so.o.x, so.o.y, so.o.z, 1e-5f);
             shd.sh_d[ps] = make_float4(so.d.x, so.d.y, so.d.z, so.dist - 1e-5f);
-            shd.sh_c[ps] = make_float4(so.c.x, so.c.y, so.c.z, 0.0f);
+            shd.sh_c[ps] = make_float4(so.c.x, so.c.y, so.c.z, __uint_as_float(so.cont));
         }
     }
 }
@@ -596,9 +619,7 @@ static void launch_shade_t(uint32_t b, const DevScene& s, const Queues& q, int g
         case kBucketLambert: k_shade<kBucketLambert, kMulti, kBlock><<<grid, kBlock, 0, st>>>(s, q); break;
         case kBucketDielectric: k_shade<kBucketDielectric, kMulti, kBlock><<<grid, kBlock, 0, st>>>(s, q); break;
         case kBucketGGX: k_shade<kBucketGGX, kMulti, kBlock><<<grid, kBlock, 0, st>>>(s, q); break;
-        case kBucketLambertResume:
-            k_shade<kBucketLambertResume, kMulti, kBlock><<<grid, kBlock, 0, st>>>(s, q);
-            break;
+        case kBucketLambertResume: break;  // continued by the shadow kernel
         default: k_shade<kBucketOther, kMulti, kBlock><<<grid, kBlock, 0, st>>>(s, q); break;
     }
 }

@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
     const PathQ in = kAnyHit ? q.shd[cur] : q.ext[cur];
     uint32_t* fetch = kAnyHit ? &c->fetchShadow.v : &c->fetchExtension.v;
     const uint32_t lane = threadIdx.x & 31u;
-    // every shadow entry resumes shading in place: the resume bucket is this queue
+    // the shadow stage continues every Lambert path it traces (statistics slot)
     if (kAnyHit && blockIdx.x == 0 && threadIdx.x == 0) c->bucket[kBucketLambertResume].v = n;
     Trav t;
     TraceGeom geo{s0.nodes, s0.tris, s0.numNodes, s0.numTris};
@@ -422,12 +422,34 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
         const bool done = active && fin;
         if (kAnyHit) {
             // Shadow stage of __raygen__trace (trace.cu:27-51): add the NEE
-            // contribution to the entry's radiance in place if nothing lies in
-            // [tmin, tmax].  The resume shade reads this queue as it stands, so the
-            // path state is not copied.
-            if (done && t.pBest == kNoHit) {
-                const float4 rd = in.rad[idx], cc = in.sh_c[idx];
-                in.rad[idx] = make_float4(rd.x + cc.x, rd.y + cc.y, rd.z + cc.z, rd.w);
+            // contribution if nothing lies in [tmin, tmax], then carry out what the
+            // Lambert shade decided for the path after its shadow ray: continue
+            // with the prepared extension ray, accumulate, or drop.
+            uint32_t cont = kContDrop, slot = 0;
+            float4 rd = make_float4(0, 0, 0, 0);
+            uint4 st = make_uint4(0, 0, 0, 0);
+            if (done) {
+                const float4 cc = in.sh_c[idx];
+                rd = in.rad[idx];
+                st = in.st[idx];
+                if (t.pBest == kNoHit) rd = make_float4(rd.x + cc.x, rd.y + cc.y, rd.z + cc.z, rd.w);
+                cont = __float_as_uint(cc.w);
+                slot = slot_of(st.w);
+                if (cont == kContAccumulate) {
+                    const Frame& f = q.req[slot];
+                    const float3 L = clamp_fireflies(make_float3(rd.x, rd.y, rd.z), f.fireflyClamp);
+                    atomicAdd(f.accum + __float_as_uint(rd.w), make_float4(L.x, L.y, L.z, 0.0f));
+                }
+            }
+            count_ended_t(q.ctl, done && cont != kContExt, slot);
+            const uint32_t pos = warp_append_pos(&c->ext[cur ^ 1u].v, done && cont == kContExt, q.capacity, &c->error);
+            if (pos != kInvalidSlot) {
+                const PathQ o = cur ? q.ext[0] : q.ext[1];
+                o.ray_o[pos] = in.ray_o[idx];
+                o.ray_d[pos] = in.ray_d[idx];
+                o.thr[pos] = in.thr[idx];
+                o.rad[pos] = rd;
+                o.st[pos] = st;
             }
         } else {
             uint32_t bucket = kNumBuckets;

@@ -14,10 +14,12 @@
 //      ray_o (origin, tmin)   ray_d (direction, tmax)   hit (t, prim, material, -)
 //      thr (throughput, prevPdf)   rad (radiance, pixel)   st (seed, rngDim, depth|iter<<16, flags)
 //      sh_o / sh_d (shadow ray)    sh_c (NEE contribution)
-//   Queues: extension (ray_o ray_d thr rad st) and shadow (all nine fields), each
-//   double-buffered across iterations, and four material buckets (ray_o ray_d hit
-//   thr rad st); Lambert paths resume from the shadow queue, whose radiance the
-//   shadow kernel updates in place.  No slot indirection and no free list: a path occupies exactly one
+//   Queues: extension (ray_o ray_d thr rad st) and shadow (the path's continuation
+//   ray_o ray_d thr rad st + sh_o sh_d sh_c), each double-buffered across
+//   iterations, and four material buckets (ray_o ray_d hit thr rad st).  A Lambert
+//   path that sends a shadow ray has already drawn its bounce and roulette; the
+//   shadow kernel adds the contribution if unoccluded and then continues the path
+//   (next extension queue), accumulates it, or drops it, as sh_c.w says.  No slot indirection and no free list: a path occupies exactly one
 //   entry between iterations, so the room for new camera paths is the capacity
 //   minus the extension and shadow entries the last iteration produced.
 #pragma once
@@ -29,9 +31,9 @@
 namespace wrk {
 
 enum : uint32_t { kLambert = 0, kEmissive = 1, kGlass = 2, kGGX = 3, kGGXT = 4 };
-// Material buckets the trace kernel sorts hits into.
-// Lambert hits that still owe their NEE light sample and Lambert paths resuming
-// after their shadow ray take separate buckets so each warp runs one branch.
+// Material buckets the trace kernel sorts hits into.  Index kBucketLambertResume
+// only counts the Lambert paths the shadow stage continues (it has no queue and
+// no shade kernel).
 enum : uint32_t {
     kBucketLambert = 0,
     kBucketDielectric = 1,
@@ -41,7 +43,11 @@ enum : uint32_t {
     kNumBuckets = 5
 };
 // st.w: flags in bits 0-7, the path's request slot in bits 8-15
-enum : uint32_t { kFlagFirstHit = 1u, kFlagPrevDelta = 2u, kFlagNeeDone = 4u };
+enum : uint32_t { kFlagFirstHit = 1u, kFlagPrevDelta = 2u };
+// What a Lambert path does after its shadow ray (sh_c.w): continue with the
+// prepared extension ray, accumulate its radiance, or end unaccumulated (the
+// iteration bound).
+enum : uint32_t { kContExt = 0u, kContAccumulate = 1u, kContDrop = 2u };
 constexpr uint32_t kSlotShift = 8;
 __host__ __device__ inline uint32_t slot_of(uint32_t stw) { return (stw >> kSlotShift) & 0xffu; }
 
