@@ -382,8 +382,12 @@ __global__ void k_small(uint32_t numSmall, const SmallTask* __restrict__ small, 
                     for (uint32_t k = 0; k < cnt; ++k) ref[it.begin + k] = ord[k];
             }
         }
-        // leaf when small enough and the split does not pay for one traversal step
-        bool leaf = cnt <= 1 || (cnt <= kMaxLeaf && (parentA <= 0.0f || (float)cnt * parentA <= parentA + bestCost));
+        // leaf when small enough and the split does not pay for a traversal step,
+        // priced at half a triangle test (SAH with Ct/Ci = 0.5: an 8-wide node test
+        // is shared by up to eight children; showcase extension traversal ran 3.5 % faster
+        // than with Ct/Ci = 1)
+        bool leaf = cnt <= 1 ||
+                    (cnt <= kMaxLeaf && (parentA <= 0.0f || (float)cnt * parentA <= 0.5f * parentA + bestCost));
         if (bestAxis < 0) leaf = cnt <= kMaxLeaf;
         if (leaf) {
             nd.left = it.begin;
