@@ -60,9 +60,8 @@ UNET_FLOP_PER_PX = sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in UNET_LAYERS)
 # Algorithmic HBM bytes per unit of work of each loop stage (per path, per ray):
 #   trace_extension: read the ray (origin|tmin, direction|tmax = 32 B) + write the
 #                    hit record (t, prim, material = 16 B)                      = 48 B / ray
-#   trace_shadow:    shadow ray 32 B + contribution 16 B + radiance 16 B + state
-#                    16 B read; the continuing path's ray and throughput (48 B) read
-#                    and its extension entry (80 B) written               = 208 B / shadow ray
+#   trace_shadow:    shadow ray 32 B + contribution 16 B read, the continuing
+#                    path's radiance 16 B read and written                 = 80 B / shadow ray
 #   shade_*:         read direction 16 + hit 16 + path state 48, write state 48 +
 #                    next ray 32                                                = 160 B / path
 # Measured DRAM traffic of the extension-ray traversal kernel per ray: ncu
@@ -71,7 +70,7 @@ UNET_FLOP_PER_PX = sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in UNET_LAYERS)
 # rays (profiles/k_trace_persistent_dram_showcase_16spp.md); traffic per launch of
 # the full workload = this x rays per launch (traffic grows with the rays traced).
 TRACE_EXT_TRAFFIC_BYTES_PER_RAY = 148.4
-STAGE_BYTES = {"trace_extension": 48, "trace_shadow": 208, "shade_lambert": 160, "shade_dielectric": 160,
+STAGE_BYTES = {"trace_extension": 48, "trace_shadow": 80, "shade_lambert": 160, "shade_dielectric": 160,
                "shade_ggx": 160, "shade_emissive": 160}
 
 
@@ -447,7 +446,7 @@ def main():
                        "parallelism": f"sample-split x{world}, one NCCL all-reduce of the frame per step"
                        if world > 1 else "single GPU",
                        "l2": f"per-step working set exceeds the 126 MB L2 (path queues: {tune['capacity']} entries "
-                             f"x 832 B = {tune['capacity'] * 832 / 1e9:.1f} GB)"},
+                             f"x 672 B = {tune['capacity'] * 672 / 1e9:.1f} GB)"},
             "mrays_per_s": mrays,
             "iterations_per_step": iters / args.steps,
             "gpu_launches": iters * 9 + args.steps * 2,

@@ -187,10 +187,10 @@ cudaError_t Engine::init(int dev, uint32_t cap) {
         return e;
     memset(hCtl, 0, sizeof(SlotCtl) * kMaxSlots);
     memset(hGenOrder, 0, sizeof(uint32_t) * (kMaxSlots + 4));
-    // SoA path queues: extension x2 (5 fields), shadow x2 (8 fields), the four
+    // SoA path queues: extension x2 (5 fields), shadow x2 (4 fields), the four
     // material buckets the extension trace fills (6 fields)
     size_t C = capacity;
-    const size_t fields = 2 * 5 + 2 * 8 + kBucketLambertResume * 6;
+    const size_t fields = 2 * 5 + 2 * 4 + kBucketLambertResume * 6;
     if ((e = queues.alloc(C * fields * sizeof(float4))) != cudaSuccess) return e;
     float4* next = queues.as<float4>();
     auto take = [&]() {
@@ -208,11 +208,7 @@ cudaError_t Engine::init(int dev, uint32_t cap) {
         x.st = reinterpret_cast<uint4*>(take());
         PathQ& h = q.shd[k];
         h = PathQ{};
-        h.ray_o = take();
-        h.ray_d = take();
-        h.thr = take();
         h.rad = take();
-        h.st = reinterpret_cast<uint4*>(take());
         h.sh_o = take();
         h.sh_d = take();
         h.sh_c = take();

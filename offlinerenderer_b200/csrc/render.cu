@@ -69,7 +69,9 @@ __global__ void k_control(Queues q) {
     uint32_t cur = c->cur ^ 1u;
     uint32_t out = cur ^ 1u;
     c->cur = cur;
-    c->ext[out].v = 0;
+    // the Lambert continuations the last iteration placed at the front of ext[out]
+    c->ext[out].v = c->cont.v;
+    c->cont.v = 0;
     c->shd[out].v = 0;
     for (int b = 0; b < kNumBuckets; ++b) c->bucket[b].v = 0;
     c->fetchExtension.v = 0;
@@ -576,6 +578,7 @@ __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k
         const uint32_t i = base + threadIdx.x;
         PathRegs r;
         ShadowOut so;
+        so.cont = kContDrop;
         int out = kOutNone;
         uint32_t slot = 0;
         if (i < n) {
@@ -592,23 +595,30 @@ __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k
         count_ended(q.ctl, out == kOutDone, slot);
         uint32_t pe = append_pos(&c->ext[nxt].v, out == kOutExt, q.capacity, &c->error);
         uint32_t ps = append_pos(&c->shd[nxt].v, out == kOutShadow, q.capacity, &c->error);
-        if (pe != kInvalidSlot) {
-            ext.ray_o[pe] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
-            ext.ray_d[pe] = make_float4(r.d.x, r.d.y, r.d.z, 1e20f);
-            ext.thr[pe] = make_float4(r.thr.x, r.thr.y, r.thr.z, r.prevPdf);
-            ext.rad[pe] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
-            ext.st[pe] = make_uint4(r.seed, r.dim, (r.depth & 0xffffu) | (r.iter << 16), r.flags);
-        } else if (ps != kInvalidSlot) {
-            if (so.cont == kContExt) {  // the extension ray the path continues with
-                shd.ray_o[ps] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
-                shd.ray_d[ps] = make_float4(r.d.x, r.d.y, r.d.z, 1e20f);
-                shd.thr[ps] = make_float4(r.thr.x, r.thr.y, r.thr.z, r.prevPdf);
-            }
-            shd.rad[ps] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
-            shd.st[ps] = make_uint4(r.seed, r.dim, (r.depth & 0xffffu) | (r.iter << 16), r.flags);
-            shd.sh_o[ps] = make_float4(so.o.x, so.o.y, so.o.z, 1e-5f);
-            shd.sh_d[ps] = make_float4(so.d.x, so.d.y, so.d.z, so.dist - 1e-5f);
-            shd.sh_c[ps] = make_float4(so.c.x, so.c.y, so.c.z, __uint_as_float(so.cont));
+        // A Lambert path that continues after its shadow ray is placed now in the
+        // extension buffer it will be traced from two iterations on (this
+        // iteration's input, no longer read); the control kernel of the next
+        // iteration starts that queue after these entries.
+        const bool cx = ps != kInvalidSlot && so.cont == kContExt;
+        const uint32_t pc = append_pos(&c->cont.v, cx, q.capacity, &c->error);
+        if (pe != kInvalidSlot || pc != kInvalidSlot) {
+            const PathQ o = pe != kInvalidSlot ? ext : (cur ? q.ext[1] : q.ext[0]);
+            const uint32_t p = pe != kInvalidSlot ? pe : pc;
+            o.ray_o[p] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
+            o.ray_d[p] = make_float4(r.d.x, r.d.y, r.d.z, 1e20f);
+            o.thr[p] = make_float4(r.thr.x, r.thr.y, r.thr.z, r.prevPdf);
+            o.rad[p] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
+            o.st[p] = make_uint4(r.seed, r.dim, (r.depth & 0xffffu) | (r.iter << 16), r.flags);
+        }
+        if (ps != kInvalidSlot) {
+            // sh_o.w: the request slot (every shadow ray starts at kShadowTmin);
+            // sh_c.w: the continuation code | the continuing path's position << 2
+            uint32_t w = so.cont;
+            if (cx) w = pc == kInvalidSlot ? (uint32_t)kContDrop : kContExt | (pc << 2);
+            if (so.cont == kContAccumulate) shd.rad[ps] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
+            shd.sh_o[ps] = make_float4(so.o.x, so.o.y, so.o.z, __uint_as_float(slot));
+            shd.sh_d[ps] = make_float4(so.d.x, so.d.y, so.d.z, so.dist - kShadowTmin);
+            shd.sh_c[ps] = make_float4(so.c.x, so.c.y, so.c.z, __uint_as_float(w));
         }
     }
 }

@@ -400,8 +400,11 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
                 if (idx < n) {
                     float4 o = kAnyHit ? in.sh_o[idx] : in.ray_o[idx];
                     float4 d = kAnyHit ? in.sh_d[idx] : in.ray_d[idx];
+                    // a shadow entry keeps its request slot where tmin would be
+                    const uint32_t slot = kAnyHit ? __float_as_uint(o.w) : slot_of(in.st[idx].w);
+                    if (kAnyHit) o.w = kShadowTmin;
                     if constexpr (kMulti) {
-                        sceneIdx = q.req[slot_of(in.st[idx].w)].scene;
+                        sceneIdx = q.req[slot].scene;
                         const DevScene& sc = q.scenes[sceneIdx];
                         geo = TraceGeom{sc.nodes, sc.tris, sc.numNodes, sc.numTris};
                     }
@@ -426,31 +429,29 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
             // Lambert shade decided for the path after its shadow ray: continue
             // with the prepared extension ray, accumulate, or drop.
             uint32_t cont = kContDrop, slot = 0;
-            float4 rd = make_float4(0, 0, 0, 0);
-            uint4 st = make_uint4(0, 0, 0, 0);
             if (done) {
                 const float4 cc = in.sh_c[idx];
-                rd = in.rad[idx];
-                st = in.st[idx];
-                if (t.pBest == kNoHit) rd = make_float4(rd.x + cc.x, rd.y + cc.y, rd.z + cc.z, rd.w);
-                cont = __float_as_uint(cc.w);
-                slot = slot_of(st.w);
-                if (cont == kContAccumulate) {
+                const uint32_t w = __float_as_uint(cc.w);
+                const bool lit = t.pBest == kNoHit;
+                cont = w & 3u;
+                slot = __float_as_uint(in.sh_o[idx].w);
+                if (cont == kContExt) {
+                    // the continuing path's entry waits in the next extension queue
+                    const uint32_t pos = w >> 2;
+                    if (lit && pos < q.capacity) {
+                        const PathQ o = cur ? q.ext[0] : q.ext[1];
+                        const float4 rd = o.rad[pos];
+                        o.rad[pos] = make_float4(rd.x + cc.x, rd.y + cc.y, rd.z + cc.z, rd.w);
+                    }
+                } else if (cont == kContAccumulate) {
+                    float4 rd = in.rad[idx];
+                    if (lit) rd = make_float4(rd.x + cc.x, rd.y + cc.y, rd.z + cc.z, rd.w);
                     const Frame& f = q.req[slot];
                     const float3 L = clamp_fireflies(make_float3(rd.x, rd.y, rd.z), f.fireflyClamp);
                     atomicAdd(f.accum + __float_as_uint(rd.w), make_float4(L.x, L.y, L.z, 0.0f));
                 }
             }
             count_ended_t(q.ctl, done && cont != kContExt, slot);
-            const uint32_t pos = warp_append_pos(&c->ext[cur ^ 1u].v, done && cont == kContExt, q.capacity, &c->error);
-            if (pos != kInvalidSlot) {
-                const PathQ o = cur ? q.ext[0] : q.ext[1];
-                o.ray_o[pos] = in.ray_o[idx];
-                o.ray_d[pos] = in.ray_d[idx];
-                o.thr[pos] = in.thr[idx];
-                o.rad[pos] = rd;
-                o.st[pos] = st;
-            }
         } else {
             uint32_t bucket = kNumBuckets;
             float4 th = make_float4(0, 0, 0, 0), rd = make_float4(0, 0, 0, 0);

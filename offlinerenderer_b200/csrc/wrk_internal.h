@@ -14,12 +14,15 @@
 //      ray_o (origin, tmin)   ray_d (direction, tmax)   hit (t, prim, material, -)
 //      thr (throughput, prevPdf)   rad (radiance, pixel)   st (seed, rngDim, depth|iter<<16, flags)
 //      sh_o / sh_d (shadow ray)    sh_c (NEE contribution)
-//   Queues: extension (ray_o ray_d thr rad st) and shadow (the path's continuation
-//   ray_o ray_d thr rad st + sh_o sh_d sh_c), each double-buffered across
+//   Queues: extension (ray_o ray_d thr rad st) and shadow (sh_o = origin | request
+//   slot, sh_d = direction | tmax, sh_c = contribution | continuation, and rad for
+//   a path that ends after its shadow ray), each double-buffered across
 //   iterations, and four material buckets (ray_o ray_d hit thr rad st).  A Lambert
-//   path that sends a shadow ray has already drawn its bounce and roulette; the
-//   shadow kernel adds the contribution if unoccluded and then continues the path
-//   (next extension queue), accumulates it, or drops it, as sh_c.w says.  No slot indirection and no free list: a path occupies exactly one
+//   path that sends a shadow ray has already drawn its bounce and roulette: if it
+//   goes on, its next extension entry is written at once (at the front of the
+//   extension buffer it will be traced from), and the shadow kernel only adds the
+//   contribution to that entry's radiance when the light is visible; otherwise
+//   the shadow kernel accumulates or drops it, as sh_c.w says.  No slot indirection and no free list: a path occupies exactly one
 //   entry between iterations, so the room for new camera paths is the capacity
 //   minus the extension and shadow entries the last iteration produced.
 #pragma once
@@ -48,6 +51,9 @@ enum : uint32_t { kFlagFirstHit = 1u, kFlagPrevDelta = 2u };
 // prepared extension ray, accumulate its radiance, or end unaccumulated (the
 // iteration bound).
 enum : uint32_t { kContExt = 0u, kContAccumulate = 1u, kContDrop = 2u };
+// Start of every shadow ray's [tmin, tmax] (the light sample's distance minus it
+// is tmax), so the queue does not store it.
+constexpr float kShadowTmin = 1e-5f;
 constexpr uint32_t kSlotShift = 8;
 __host__ __device__ inline uint32_t slot_of(uint32_t stw) { return (stw >> kSlotShift) & 0xffu; }
 
@@ -119,6 +125,7 @@ struct Counters {
     HotCounter ext[2];
     HotCounter shd[2];
     HotCounter bucket[kNumBuckets];
+    HotCounter cont;            // Lambert continuations placed in ext[cur] this iteration
     HotCounter fetchExtension;  // rays taken by the persistent traversal kernels this iteration
     HotCounter fetchShadow;
     uint32_t cur;          // which ext/shd buffer the current iteration consumes
