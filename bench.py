@@ -65,11 +65,11 @@ UNET_FLOP_PER_PX = sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in UNET_LAYERS)
 #   shade_*:         read direction 16 + hit 16 + path state 48, write state 48 +
 #                    next ray 32                                                = 160 B / path
 # Measured DRAM traffic of the extension-ray traversal kernel per ray: ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum) summed over all 64 launches of four
-# 512x512 16-spp renders of the same scene, divided by their 57,625,904 extension
-# rays (profiles/k_trace_persistent_dram_showcase_16spp.md); traffic per launch of
+# (dram__bytes_read.sum + dram__bytes_write.sum) summed over the 12 launches of the
+# 512x512 16-spp render of the same scene that ncu profiles (the plain-launch,
+# stage-timed one), divided by its 14,406,476 extension rays; traffic per launch of
 # the full workload = this x rays per launch (traffic grows with the rays traced).
-TRACE_EXT_TRAFFIC_BYTES_PER_RAY = 148.4
+TRACE_EXT_TRAFFIC_BYTES_PER_RAY = 148.5
 STAGE_BYTES = {"trace_extension": 48, "trace_shadow": 80, "shade_lambert": 160, "shade_dielectric": 160,
                "shade_ggx": 160, "shade_emissive": 160}
 
