@@ -70,6 +70,10 @@ UNET_FLOP_PER_PX = sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in UNET_LAYERS)
 # stage-timed one), divided by its 14,406,476 extension rays; traffic per launch of
 # the full workload = this x rays per launch (traffic grows with the rays traced).
 TRACE_EXT_TRAFFIC_BYTES_PER_RAY = 148.5
+# SM issue-slot utilisation of the traversal and shading kernels (the roofline that
+# bounds them: SIMT integer / FP32 work, not HBM), smsp__issue_active from ncu --set
+# full on the 16-spp capture of the same scene.  CUDA events cannot measure it live.
+STAGE_ISSUE_ACTIVE = {"trace_extension": 0.710, "trace_shadow": 0.600, "shade_lambert": 0.566}
 STAGE_BYTES = {"trace_extension": 48, "trace_shadow": 80, "shade_lambert": 160, "shade_dielectric": 160,
                "shade_ggx": 160, "shade_emissive": 160}
 
@@ -462,6 +466,7 @@ def main():
                          "units_per_launch": units[dominant] / launches},
             "stage_ms": stage_ms,
             "stage_algorithmic_gbs": stage_gbs,
+            "stage_sm_issue_active": dict(STAGE_ISSUE_ACTIVE, source="ncu smsp__issue_active, 16-spp capture"),
             "stage_units": units,
             "clocks": clk,
             "cpu_baseline": cpu,

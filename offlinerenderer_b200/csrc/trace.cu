@@ -12,8 +12,9 @@
 // shared memory, spilling to a bounded local array; overflow raises an error bit
 // and ends the ray instead of corrupting memory.
 //
-// The triangle test is Moller-Trumbore written with _rn intrinsics so the FP32
-// result is the same sequence of correctly rounded operations as the CPU oracle's.
+// The triangle test is Moller-Trumbore written with _rn / fmaf intrinsics so the
+// FP32 result is the same sequence of correctly rounded operations as the CPU
+// oracle's.
 #include "wrk_internal.h"
 #include "wrk_shading.cuh"
 
@@ -29,23 +30,25 @@ struct Ray {
 };
 
 // Moller-Trumbore without the reciprocal: barycentric numerators are compared
-// with det (sign-aware) and t is divided only for hits inside the triangle.
+// with det (sign-aware) and t is divided only for hits inside the triangle.  Each
+// cross-product component is one product and one FMA, each dot product one product
+// and two FMAs (correctly rounded intrinsics, in the CPU oracle's exact order).
 __device__ __forceinline__ bool mt_rn(const Ray& r, float4 a, float4 b, float4 c, float& t) {
-    float px = __fsub_rn(__fmul_rn(r.dy, c.z), __fmul_rn(r.dz, c.y));
-    float py = __fsub_rn(__fmul_rn(r.dz, c.x), __fmul_rn(r.dx, c.z));
-    float pz = __fsub_rn(__fmul_rn(r.dx, c.y), __fmul_rn(r.dy, c.x));
-    float det = __fadd_rn(__fadd_rn(__fmul_rn(b.x, px), __fmul_rn(b.y, py)), __fmul_rn(b.z, pz));
+    float px = __fmaf_rn(r.dy, c.z, -__fmul_rn(r.dz, c.y));
+    float py = __fmaf_rn(r.dz, c.x, -__fmul_rn(r.dx, c.z));
+    float pz = __fmaf_rn(r.dx, c.y, -__fmul_rn(r.dy, c.x));
+    float det = __fmaf_rn(b.x, px, __fmaf_rn(b.y, py, __fmul_rn(b.z, pz)));
     float sx = __fsub_rn(r.ox, a.x), sy = __fsub_rn(r.oy, a.y), sz = __fsub_rn(r.oz, a.z);
-    float un = __fadd_rn(__fadd_rn(__fmul_rn(sx, px), __fmul_rn(sy, py)), __fmul_rn(sz, pz));
-    float qx = __fsub_rn(__fmul_rn(sy, b.z), __fmul_rn(sz, b.y));
-    float qy = __fsub_rn(__fmul_rn(sz, b.x), __fmul_rn(sx, b.z));
-    float qz = __fsub_rn(__fmul_rn(sx, b.y), __fmul_rn(sy, b.x));
-    float vn = __fadd_rn(__fadd_rn(__fmul_rn(r.dx, qx), __fmul_rn(r.dy, qy)), __fmul_rn(r.dz, qz));
+    float un = __fmaf_rn(sx, px, __fmaf_rn(sy, py, __fmul_rn(sz, pz)));
+    float qx = __fmaf_rn(sy, b.z, -__fmul_rn(sz, b.y));
+    float qy = __fmaf_rn(sz, b.x, -__fmul_rn(sx, b.z));
+    float qz = __fmaf_rn(sx, b.y, -__fmul_rn(sy, b.x));
+    float vn = __fmaf_rn(r.dx, qx, __fmaf_rn(r.dy, qy, __fmul_rn(r.dz, qz)));
     float uv = __fadd_rn(un, vn);
     bool inside = det > 0.0f ? (un >= 0.0f && vn >= 0.0f && uv <= det)
                              : (det < 0.0f && un <= 0.0f && vn <= 0.0f && uv >= det);
     if (!inside) return false;
-    t = __fdiv_rn(__fadd_rn(__fadd_rn(__fmul_rn(c.x, qx), __fmul_rn(c.y, qy)), __fmul_rn(c.z, qz)), det);
+    t = __fdiv_rn(__fmaf_rn(c.x, qx, __fmaf_rn(c.y, qy, __fmul_rn(c.z, qz))), det);
     return true;
 }
 

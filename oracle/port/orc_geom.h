@@ -225,26 +225,30 @@ inline void build_bvh(Scene& s) {
 
 // Moller-Trumbore, FP32, without the reciprocal: the barycentric tests compare the
 // numerators u*det and v*det against det (sign-aware), and t = t_num / det is
-// divided (correctly rounded) only for hits inside the triangle.  The CUDA trace
-// kernel evaluates the same expression sequence on the same per-triangle
-// (v0, v1-v0, v2-v0) values, so t is bit-identical.
-inline bool mt32(const float o[3], const float d[3], const float* v0, const float* e1, const float* e2,
-                        float& t) {
-    float px = d[1] * e2[2] - d[2] * e2[1];
-    float py = d[2] * e2[0] - d[0] * e2[2];
-    float pz = d[0] * e2[1] - d[1] * e2[0];
-    float det = e1[0] * px + e1[1] * py + e1[2] * pz;
+// divided (correctly rounded) only for hits inside the triangle.  Cross-product
+// components are a product and one fused multiply-add, dot products a product and
+// two (std::fma is correctly rounded, as the GPU's fmaf).  The CUDA trace kernel
+// evaluates the same operation sequence on the same per-triangle (v0, v1-v0,
+// v2-v0) values, so t is bit-identical.  Built twice (GCC target clones): with
+// the host's FMA instruction where the CPU has one, else through libm's fmaf; both
+// give the same correctly rounded results.
+__attribute__((target_clones("fma", "default"))) static bool mt32(const float o[3], const float d[3], const float* v0,
+                                                                 const float* e1, const float* e2, float& t) {
+    float px = std::fma(d[1], e2[2], -(d[2] * e2[1]));
+    float py = std::fma(d[2], e2[0], -(d[0] * e2[2]));
+    float pz = std::fma(d[0], e2[1], -(d[1] * e2[0]));
+    float det = std::fma(e1[0], px, std::fma(e1[1], py, e1[2] * pz));
     if (det == 0.0f) return false;
     float sx = o[0] - v0[0], sy = o[1] - v0[1], sz = o[2] - v0[2];
-    float un = sx * px + sy * py + sz * pz;
-    float qx = sy * e1[2] - sz * e1[1];
-    float qy = sz * e1[0] - sx * e1[2];
-    float qz = sx * e1[1] - sy * e1[0];
-    float vn = d[0] * qx + d[1] * qy + d[2] * qz;
+    float un = std::fma(sx, px, std::fma(sy, py, sz * pz));
+    float qx = std::fma(sy, e1[2], -(sz * e1[1]));
+    float qy = std::fma(sz, e1[0], -(sx * e1[2]));
+    float qz = std::fma(sx, e1[1], -(sy * e1[0]));
+    float vn = std::fma(d[0], qx, std::fma(d[1], qy, d[2] * qz));
     float uv = un + vn;
     bool inside = det > 0.0f ? (un >= 0.0f && vn >= 0.0f && uv <= det) : (un <= 0.0f && vn <= 0.0f && uv >= det);
     if (!inside) return false;
-    t = (e2[0] * qx + e2[1] * qy + e2[2] * qz) / det;
+    t = std::fma(e2[0], qx, std::fma(e2[1], qy, e2[2] * qz)) / det;
     return true;
 }
 
