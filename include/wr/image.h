@@ -10,5 +10,9 @@
 namespace test_helpers {
 
 void savePNG(const char* filename, const wr::Vec3* image, uint32_t width, uint32_t height);
+// Additive: the linear radiance as an OpenEXR (32-bit float B G R) or Radiance
+// RGBE file, no tone map.
+void saveEXR(const char* filename, const wr::Vec3* image, uint32_t width, uint32_t height);
+void saveHDR(const char* filename, const wr::Vec3* image, uint32_t width, uint32_t height);
 
 }  // namespace test_helpers

@@ -288,6 +288,13 @@ int wrk_tonemap_aces(const float* d_rgb, uint32_t numPixels, uint8_t* d_out);
 int wrk_image_save_png(const char* path, const float* rgb, uint32_t width, uint32_t height);
 /* Writes host RGB8 bytes (width*height*3) as a PNG file (zlib deflate); 0 on success. */
 int wrk_png_write(const char* path, const uint8_t* rgb8, uint32_t width, uint32_t height);
+/* HDR outputs of linear host float RGB (width*height*3, rows top to bottom), no tone
+ * map (the next step after accumulation; libWR writes only the 8-bit PNG of
+ * libWR/test/helpers/image.cpp:23-49):
+ * OpenEXR 2 scan-line file, uncompressed, channels B G R as 32-bit float. */
+int wrk_exr_write(const char* path, const float* rgb, uint32_t width, uint32_t height);
+/* Radiance .hdr (RGBE, run-length scan lines for 8 <= width < 32768, else flat). */
+int wrk_hdr_write(const char* path, const float* rgb, uint32_t width, uint32_t height);
 
 /* ---- learned denoiser: replaces the OptiX AI denoiser of libWR
  *      (libWR/src/internal/denoiser.cpp:17-195: optixDenoiserCreate :30-35,

@@ -9,6 +9,8 @@
 // (libWR/src/internal/cuda_utils.h:13-39).
 #include <zlib.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -563,9 +565,139 @@ extern "C" int wrk_image_save_png(const char* path, const float* rgb, uint32_t w
     return wrk_png_write(path, bytes.data(), width, height);
 }
 
+// ---------------------------------------------------------------------------
+// HDR outputs of the linear radiance (no tone map): OpenEXR and Radiance RGBE.
+namespace {
+
+void put_le32(std::vector<uint8_t>& o, uint32_t v) {
+    for (int k = 0; k < 4; ++k) o.push_back((uint8_t)(v >> (8 * k)));
+}
+void put_le64(std::vector<uint8_t>& o, uint64_t v) {
+    for (int k = 0; k < 8; ++k) o.push_back((uint8_t)(v >> (8 * k)));
+}
+void put_f32(std::vector<uint8_t>& o, float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    put_le32(o, u);
+}
+void put_cstr(std::vector<uint8_t>& o, const char* s) { o.insert(o.end(), s, s + std::strlen(s) + 1); }
+// One header attribute: name, type name, byte size, value.
+void put_attr(std::vector<uint8_t>& o, const char* name, const char* type, const std::vector<uint8_t>& v) {
+    put_cstr(o, name);
+    put_cstr(o, type);
+    put_le32(o, (uint32_t)v.size());
+    o.insert(o.end(), v.begin(), v.end());
+}
+
+int write_file(const char* path, const std::vector<uint8_t>& bytes, const char* what) {
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return wrk::report_error(WRK_ERR_INVALID, (std::string(what) + ": cannot open " + path).c_str());
+    const bool ok = std::fwrite(bytes.data(), 1, bytes.size(), f) == bytes.size();
+    std::fclose(f);
+    return ok ? WRK_OK : wrk::report_error(WRK_ERR_INVALID, (std::string(what) + ": write failed").c_str());
+}
+
+// Radiance RGBE of one pixel (Ward's shared-exponent encoding): the largest
+// component's binary exponent e is shared, mantissas scaled by 256 / 2^e.
+void rgbe(const float* c, uint8_t* out) {
+    const float v = std::max(c[0], std::max(c[1], c[2]));
+    if (!(v >= 1e-32f)) {  // also NaN
+        out[0] = out[1] = out[2] = out[3] = 0;
+        return;
+    }
+    int e;
+    const float m = std::frexp(v, &e);  // v = m * 2^e, m in [0.5, 1)
+    const float scale = m * 256.0f / v;
+    for (int k = 0; k < 3; ++k) out[k] = (uint8_t)std::max(0.0f, c[k] * scale);
+    out[3] = (uint8_t)(e + 128);
+}
+
+}  // namespace
+
+extern "C" int wrk_exr_write(const char* path, const float* rgb, uint32_t width, uint32_t height) {
+    if (!path || !rgb || width == 0 || height == 0 || width > (1u << 30) / 12 || height > (1u << 30))
+        return wrk::report_error(WRK_ERR_INVALID, "exr: bad arguments");
+    // OpenEXR 2 single-part scan-line file, no compression, one scan line per
+    // block, channels B G R (alphabetical, as the format requires) as 32-bit float.
+    std::vector<uint8_t> o = {0x76, 0x2f, 0x31, 0x01};
+    put_le32(o, 2u);
+    std::vector<uint8_t> ch;
+    for (const char* name : {"B", "G", "R"}) {
+        put_cstr(ch, name);
+        put_le32(ch, 2u);                          // pixel type FLOAT
+        ch.push_back(0);                           // pLinear
+        ch.push_back(0), ch.push_back(0), ch.push_back(0);
+        put_le32(ch, 1u);                          // x sampling
+        put_le32(ch, 1u);                          // y sampling
+    }
+    ch.push_back(0);
+    put_attr(o, "channels", "chlist", ch);
+    put_attr(o, "compression", "compression", {0});
+    std::vector<uint8_t> win;
+    put_le32(win, 0), put_le32(win, 0), put_le32(win, width - 1), put_le32(win, height - 1);
+    put_attr(o, "dataWindow", "box2i", win);
+    put_attr(o, "displayWindow", "box2i", win);
+    put_attr(o, "lineOrder", "lineOrder", {0});
+    std::vector<uint8_t> one;
+    put_f32(one, 1.0f);
+    put_attr(o, "pixelAspectRatio", "float", one);
+    std::vector<uint8_t> ctr;
+    put_f32(ctr, 0.0f), put_f32(ctr, 0.0f);
+    put_attr(o, "screenWindowCenter", "v2f", ctr);
+    put_attr(o, "screenWindowWidth", "float", one);
+    o.push_back(0);  // end of header
+    const uint64_t rowBytes = 12ull * width, blockBytes = 8 + rowBytes;
+    const uint64_t first = o.size() + 8ull * height;
+    for (uint32_t y = 0; y < height; ++y) put_le64(o, first + y * blockBytes);
+    o.reserve(first + height * blockBytes);
+    for (uint32_t y = 0; y < height; ++y) {
+        put_le32(o, y);
+        put_le32(o, (uint32_t)rowBytes);
+        const float* row = rgb + (size_t)y * 3 * width;
+        for (int c = 2; c >= 0; --c)  // B, G, R planes of the scan line
+            for (uint32_t x = 0; x < width; ++x) put_f32(o, row[3 * x + c]);
+    }
+    return write_file(path, o, "exr");
+}
+
+extern "C" int wrk_hdr_write(const char* path, const float* rgb, uint32_t width, uint32_t height) {
+    if (!path || !rgb || width == 0 || height == 0) return wrk::report_error(WRK_ERR_INVALID, "hdr: bad arguments");
+    std::string head = "#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n-Y " + std::to_string(height) + " +X " +
+                       std::to_string(width) + "\n";
+    std::vector<uint8_t> o(head.begin(), head.end());
+    std::vector<uint8_t> px(4 * (size_t)width);
+    const bool rle = width >= 8 && width < 32768;
+    for (uint32_t y = 0; y < height; ++y) {
+        for (uint32_t x = 0; x < width; ++x) rgbe(rgb + 3 * ((size_t)y * width + x), &px[4 * (size_t)x]);
+        if (!rle) {  // flat scan line (the run-length form needs 8 <= width < 32768)
+            o.insert(o.end(), px.begin(), px.end());
+            continue;
+        }
+        // run-length form: marker 2 2 width, then each component plane as literal
+        // runs of at most 128 bytes (count byte, bytes)
+        o.push_back(2), o.push_back(2), o.push_back((uint8_t)(width >> 8)), o.push_back((uint8_t)width);
+        for (int c = 0; c < 4; ++c)
+            for (uint32_t x = 0; x < width;) {
+                const uint32_t n = std::min<uint32_t>(128, width - x);
+                o.push_back((uint8_t)n);
+                for (uint32_t k = 0; k < n; ++k) o.push_back(px[4 * (size_t)(x + k) + c]);
+                x += n;
+            }
+    }
+    return write_file(path, o, "hdr");
+}
+
 namespace test_helpers {
 void savePNG(const char* filename, const wr::Vec3* image, uint32_t width, uint32_t height) {
     int rc = wrk_image_save_png(filename, reinterpret_cast<const float*>(image), width, height);
     if (rc) throw std::runtime_error(std::string("savePNG(") + (filename ? filename : "") + "): " + wrk_last_error());
+}
+void saveEXR(const char* filename, const wr::Vec3* image, uint32_t width, uint32_t height) {
+    int rc = wrk_exr_write(filename, reinterpret_cast<const float*>(image), width, height);
+    if (rc) throw std::runtime_error(std::string("saveEXR(") + (filename ? filename : "") + "): " + wrk_last_error());
+}
+void saveHDR(const char* filename, const wr::Vec3* image, uint32_t width, uint32_t height) {
+    int rc = wrk_hdr_write(filename, reinterpret_cast<const float*>(image), width, height);
+    if (rc) throw std::runtime_error(std::string("saveHDR(") + (filename ? filename : "") + "): " + wrk_last_error());
 }
 }  // namespace test_helpers

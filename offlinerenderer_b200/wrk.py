@@ -132,6 +132,8 @@ SIGNATURES = {
     "wrk_tonemap_aces": ([_VP, _U32, _VP], _I),
     "wrk_image_save_png": ([C.c_char_p, _VP, _U32, _U32], _I),
     "wrk_png_write": ([C.c_char_p, _VP, _U32, _U32], _I),
+    "wrk_exr_write": ([C.c_char_p, _VP, _U32, _U32], _I),
+    "wrk_hdr_write": ([C.c_char_p, _VP, _U32, _U32], _I),
     "wrk_renderer_set_launch": ([_VP, _U32, _U32], _I),
     "wrk_server_create": ([_I, _VP, C.POINTER(_VP)], _I),
     "wrk_server_destroy": ([_VP], _I),
@@ -735,6 +737,20 @@ def autotune(scene: Scene, camera=None, settings=None, spp=None, device: int = 0
     _check(lib().wrk_autotune(device, scene.handle, C.byref(cam), C.byref(p), C.byref(r)))
     return {"capacity": r.capacity, "chunk": r.chunk, "shadeBlock": r.shadeBlock, "bestMs": r.bestMs,
             "trials": [_struct_dict(r.trials[i]) for i in range(r.numTrials)]}
+
+
+def save_exr(path: str, rgb: np.ndarray) -> None:
+    """Write an (H, W, 3) float image as an uncompressed 32-bit float OpenEXR file."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    h, w = rgb.shape[:2]
+    _check(lib().wrk_exr_write(os.fsencode(path), rgb.ctypes.data, w, h))
+
+
+def save_hdr(path: str, rgb: np.ndarray) -> None:
+    """Write an (H, W, 3) float image as a Radiance RGBE (.hdr) file."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    h, w = rgb.shape[:2]
+    _check(lib().wrk_hdr_write(os.fsencode(path), rgb.ctypes.data, w, h))
 
 
 def save_png(path: str, rgb: np.ndarray) -> None:
