@@ -229,11 +229,12 @@ inline void build_bvh(Scene& s) {
 // components are a product and one fused multiply-add, dot products a product and
 // two (std::fma is correctly rounded, as the GPU's fmaf).  The CUDA trace kernel
 // evaluates the same operation sequence on the same per-triangle (v0, v1-v0,
-// v2-v0) values, so t is bit-identical.  Built twice (GCC target clones): with
-// the host's FMA instruction where the CPU has one, else through libm's fmaf; both
-// give the same correctly rounded results.
-__attribute__((target_clones("fma", "default"))) static bool mt32(const float o[3], const float d[3], const float* v0,
-                                                                 const float* e1, const float* e2, float& t) {
+// v2-v0) values, so t is bit-identical.  Inlined into the traversal routines,
+// which are built twice (GCC target clones): with the host's FMA instruction where
+// the CPU has one, else through libm's fmaf; both give the same correctly rounded
+// results.
+__attribute__((always_inline)) inline bool mt32(const float o[3], const float d[3], const float* v0, const float* e1,
+                                                const float* e2, float& t) {
     float px = std::fma(d[1], e2[2], -(d[2] * e2[1]));
     float py = std::fma(d[2], e2[0], -(d[0] * e2[2]));
     float pz = std::fma(d[0], e2[1], -(d[1] * e2[0]));
@@ -286,8 +287,9 @@ inline bool box_hit(const BNode& b, const float o[3], const float inv[3], float 
 }
 
 // Closest hit over [tmin, tmax]; ties in t go to the lower triangle index.
-inline bool closest32(const Scene& s, const float o[3], const float d[3], float tmin, float tmax, float& tb,
-                      uint32_t& pb) {
+__attribute__((target_clones("fma", "default"))) static bool closest32(const Scene& s, const float o[3],
+                                                                      const float d[3], float tmin, float tmax,
+                                                                      float& tb, uint32_t& pb) {
     float inv[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};
     tb = tmax;
     pb = 0xffffffffu;
@@ -315,7 +317,8 @@ inline bool closest32(const Scene& s, const float o[3], const float d[3], float 
     return pb != 0xffffffffu;
 }
 
-inline bool occluded32(const Scene& s, const float o[3], const float d[3], float tmin, float tmax) {
+__attribute__((target_clones("fma", "default"))) static bool occluded32(const Scene& s, const float o[3],
+                                                                       const float d[3], float tmin, float tmax) {
     float inv[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};
     uint32_t st[128];
     int sp = 0;
