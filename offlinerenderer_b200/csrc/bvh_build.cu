@@ -4,7 +4,8 @@
 //
 // Binary build, level by level over all open tasks at once:
 //   bin     -- every primitive adds its AABB to its task's 16 bins on each axis
-//              (global atomics on order-preserving integer encodings of floats)
+//              (atomics on order-preserving integer encodings of floats, merged per
+//              block in shared memory when the block lies in one task)
 //   split   -- one thread per task sweeps the 3x15 candidate planes for the lowest
 //              SAH cost (object median when all centroids share a bin); allocates the
 //              two children; children of <= kSmallTask primitives go to the small list
@@ -141,10 +142,58 @@ __device__ __forceinline__ int bin_of(float c, float lo, float ext) {
     return min(kBins - 1, max(0, b));
 }
 
+// A block's primitives occupy consecutive positions and a task's primitives one
+// contiguous range, so when the block's first and last positions share an open
+// task, all of them do.  The block then merges into shared-memory copies of the
+// task's bins / child boxes first and each field takes one global atomic per block
+// instead of one per primitive (near the root every primitive of the scene would
+// otherwise hit the same few addresses).  min / max / add give the same result in
+// any order, so the tree does not change.
+__device__ __forceinline__ int block_task(uint32_t n, const int* __restrict__ taskOf) {
+    const uint32_t i0 = blockIdx.x * blockDim.x, i1 = min(n, i0 + blockDim.x) - 1;
+    const int a = taskOf[i0], b = taskOf[i1];
+    return a >= 0 && a == b ? a : -1;
+}
+
 __global__ void k_bin(uint32_t n, const uint32_t* __restrict__ ref, const int* __restrict__ taskOf,
                       const OBox* __restrict__ tcen, const float4* __restrict__ blo, const float4* __restrict__ bhi,
                       Bin* bins) {
+    __shared__ uint32_t sCnt[3 * kBins], sLo[3 * kBins][3], sHi[3 * kBins][3];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int bt = block_task(n, taskOf);
+    if (bt >= 0) {
+        for (uint32_t k = threadIdx.x; k < 3 * kBins; k += blockDim.x) {
+            sCnt[k] = 0;
+            for (int c = 0; c < 3; ++c) { sLo[k][c] = 0xffffffffu; sHi[k][c] = 0u; }
+        }
+        __syncthreads();
+        if (i < n) {
+            const uint32_t p = ref[i];
+            const float4 l = blo[p], h = bhi[p];
+            const float lo[3] = {l.x, l.y, l.z}, hi[3] = {h.x, h.y, h.z};
+            const OBox cb = tcen[bt];
+            for (int a = 0; a < 3; ++a) {
+                const float cl = o2f(cb.lo[a]), ch = o2f(cb.hi[a]);
+                const int k = a * kBins + bin_of(0.5f * (lo[a] + hi[a]), cl, ch - cl);
+                atomicAdd(&sCnt[k], 1u);
+                for (int c = 0; c < 3; ++c) {
+                    atomicMin(&sLo[k][c], f2o(lo[c]));
+                    atomicMax(&sHi[k][c], f2o(hi[c]));
+                }
+            }
+        }
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < 3 * kBins; k += blockDim.x) {
+            if (!sCnt[k]) continue;
+            Bin* bn = bins + (size_t)bt * 3 * kBins + k;
+            atomicAdd(&bn->cnt, sCnt[k]);
+            for (int c = 0; c < 3; ++c) {
+                atomicMin(&bn->lo[c], sLo[k][c]);
+                atomicMax(&bn->hi[c], sHi[k][c]);
+            }
+        }
+        return;
+    }
     if (i >= n) return;
     int t = taskOf[i];
     if (t < 0) return;
@@ -275,36 +324,74 @@ __global__ void k_scatter(uint32_t n, const uint32_t* __restrict__ ref, const in
                           const Split* __restrict__ splits, const float4* __restrict__ blo,
                           const float4* __restrict__ bhi, const uint32_t* __restrict__ flags,
                           const uint32_t* __restrict__ scan, uint32_t* ref2, int* taskOf2, OBox* nextCen, OBox* nbox) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int t = taskOf[i];
-    uint32_t p = ref[i];
-    if (t < 0) {
-        ref2[i] = p;
-        taskOf2[i] = -1;
-        return;
+    // [side][lo xyz | hi xyz] of the two children's boxes and centroid bounds when
+    // the block lies in one task (block_task); otherwise global atomics per primitive
+    __shared__ uint32_t sBox[2][6], sCen[2][6];
+    const int bt = block_task(n, taskOf);
+    if (bt >= 0) {
+        if (threadIdx.x < 24) {
+            const uint32_t side = threadIdx.x / 12, k = threadIdx.x % 12;
+            (k < 6 ? sBox[side][k] : sCen[side][k - 6]) = (k % 6) < 3 ? 0xffffffffu : 0u;
+        }
+        __syncthreads();
     }
-    Task tk = tasks[t];
-    Split sp = splits[t];
-    uint32_t base = scan[tk.begin];
-    uint32_t lr = scan[i] - base;
-    bool left = flags[i] != 0;
-    uint32_t np = left ? tk.begin + lr : tk.begin + sp.nLeft + ((i - tk.begin) - lr);
-    ref2[np] = p;
-    int nt = left ? sp.leftTask : sp.rightTask;
-    taskOf2[np] = nt;
-    uint32_t node = sp.leftNode + (left ? 0 : 1);
-    float4 l = blo[p], h = bhi[p];
-    float lo[3] = {l.x, l.y, l.z}, hi[3] = {h.x, h.y, h.z};
-    for (int k = 0; k < 3; ++k) {
-        atomicMin(&nbox[node].lo[k], f2o(lo[k]));
-        atomicMax(&nbox[node].hi[k], f2o(hi[k]));
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int t = taskOf[i];
+        const uint32_t p = ref[i];
+        if (t < 0) {
+            ref2[i] = p;
+            taskOf2[i] = -1;
+        } else {
+            const Task tk = tasks[t];
+            const Split sp = splits[t];
+            const uint32_t base = scan[tk.begin];
+            const uint32_t lr = scan[i] - base;
+            const bool left = flags[i] != 0;
+            const uint32_t np = left ? tk.begin + lr : tk.begin + sp.nLeft + ((i - tk.begin) - lr);
+            ref2[np] = p;
+            const int nt = left ? sp.leftTask : sp.rightTask;
+            taskOf2[np] = nt;
+            const uint32_t node = sp.leftNode + (left ? 0 : 1);
+            const float4 l = blo[p], h = bhi[p];
+            const float lo[3] = {l.x, l.y, l.z}, hi[3] = {h.x, h.y, h.z};
+            uint32_t* bx = bt >= 0 ? sBox[left ? 0 : 1] : nullptr;
+            uint32_t* cx = bt >= 0 ? sCen[left ? 0 : 1] : nullptr;
+            for (int k = 0; k < 3; ++k) {
+                atomicMin(bx ? &bx[k] : &nbox[node].lo[k], f2o(lo[k]));
+                atomicMax(bx ? &bx[3 + k] : &nbox[node].hi[k], f2o(hi[k]));
+            }
+            if (nt >= 0) {
+                for (int k = 0; k < 3; ++k) {
+                    const float c = 0.5f * (lo[k] + hi[k]);
+                    atomicMin(cx ? &cx[k] : &nextCen[nt].lo[k], f2o(c));
+                    atomicMax(cx ? &cx[3 + k] : &nextCen[nt].hi[k], f2o(c));
+                }
+            }
+        }
     }
-    if (nt >= 0) {
-        for (int k = 0; k < 3; ++k) {
-            float c = 0.5f * (lo[k] + hi[k]);
-            atomicMin(&nextCen[nt].lo[k], f2o(c));
-            atomicMax(&nextCen[nt].hi[k], f2o(c));
+    if (bt >= 0) {
+        __syncthreads();
+        if (threadIdx.x < 24) {
+            const uint32_t side = threadIdx.x / 12, k = threadIdx.x % 12;
+            const Split sp = splits[bt];
+            const bool lo = (k % 6) < 3;
+            const uint32_t v = k < 6 ? sBox[side][k] : sCen[side][k - 6];
+            const bool any = v != (lo ? 0xffffffffu : 0u);  // the side received a primitive
+            if (any) {
+                uint32_t* dst;
+                if (k < 6) {
+                    OBox& o = nbox[sp.leftNode + side];
+                    dst = lo ? &o.lo[k % 3] : &o.hi[k % 3];
+                } else {
+                    const int nt = side ? sp.rightTask : sp.leftTask;
+                    dst = nt >= 0 ? (lo ? &nextCen[nt].lo[k % 3] : &nextCen[nt].hi[k % 3]) : nullptr;
+                }
+                if (dst) {
+                    if (lo) atomicMin(dst, v);
+                    else atomicMax(dst, v);
+                }
+            }
         }
     }
 }
