@@ -21,6 +21,7 @@
 // into leaf order as (v0|prim, v1-v0|material, v2-v0) records.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -662,6 +663,43 @@ __global__ void k_collapse(uint32_t count, const CItem* __restrict__ items, cons
 
 inline unsigned grid_for(uint64_t n, unsigned b) { return (unsigned)((n + b - 1) / b); }
 
+// SAH cost of the 8-wide tree: one node test for the root plus, for every child
+// box, its surface area over the root's times the work a ray entering it does
+// (one node test, or the leaf's triangle tests).  One thread per node decodes the
+// node's quantized child boxes; sums[0] += area x work, sums[1] = the root's area
+// (the union of its children).
+__global__ void k_sah(const uint4* __restrict__ nodes, uint32_t numNodes, double* sums) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= numNodes) return;
+    const uint4* n = nodes + 5 * (size_t)i;
+    const uint4 n0 = n[0], n1 = n[1], n2 = n[2], n3 = n[3], n4 = n[4];
+    const float p[3] = {__uint_as_float(n0.x), __uint_as_float(n0.y), __uint_as_float(n0.z)};
+    float sc[3];
+    for (int a = 0; a < 3; ++a) sc[a] = ldexpf(1.0f, (int)((n0.w >> (8 * a)) & 0xffu) - 127);
+    const uint32_t imask = n0.w >> 24;
+    const uint32_t qlo[3][2] = {{n2.x, n2.y}, {n2.z, n2.w}, {n3.x, n3.y}};
+    const uint32_t qhi[3][2] = {{n3.z, n3.w}, {n4.x, n4.y}, {n4.z, n4.w}};
+    float ulo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, uhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    double acc = 0.0;
+    for (int s = 0; s < 8; ++s) {
+        float lo[3], hi[3];
+        bool empty = false;
+        for (int a = 0; a < 3; ++a) {
+            const uint32_t bl = (qlo[a][s >> 2] >> (8 * (s & 3))) & 0xffu, bh = (qhi[a][s >> 2] >> (8 * (s & 3))) & 0xffu;
+            if (bl > bh) empty = true;
+            lo[a] = p[a] + (float)bl * sc[a];
+            hi[a] = p[a] + (float)bh * sc[a];
+        }
+        if (empty) continue;
+        const uint32_t meta = ((s < 4 ? n1.z : n1.w) >> (8 * (s & 3))) & 0xffu;
+        const double work = ((imask >> s) & 1u) ? 1.0 : (double)((meta >> 5) + 1u);
+        acc += (double)half_area(lo, hi) * work;
+        for (int a = 0; a < 3; ++a) { ulo[a] = fminf(ulo[a], lo[a]); uhi[a] = fmaxf(uhi[a], hi[a]); }
+    }
+    atomicAdd(&sums[0], acc);
+    if (i == 0) sums[1] = (double)half_area(ulo, uhi);
+}
+
 }  // namespace
 
 #define WRK_BCHECK(x)                                                                               \
@@ -709,7 +747,7 @@ int build_bvh8(const float* d_vtx, const uint32_t* d_idx, const uint32_t* d_triM
     WRK_BCHECK(cudaMalloc(&ref, sizeof(uint32_t) * n));
     WRK_BCHECK(cudaMalloc(&ref2, sizeof(uint32_t) * n));
     WRK_BCHECK(cudaMalloc(&flags, sizeof(uint32_t) * n));
-    WRK_BCHECK(cudaMalloc(&scan, sizeof(uint32_t) * n));
+    WRK_BCHECK(cudaMalloc(&scan, sizeof(uint32_t) * std::max<uint32_t>(n, 4u)));  // also the SAH sums (2 doubles)
     WRK_BCHECK(cudaMalloc(&taskOf, sizeof(int) * n));
     WRK_BCHECK(cudaMalloc(&taskOf2, sizeof(int) * n));
     WRK_BCHECK(cudaMalloc(&tasks, sizeof(Task) * maxTasks));
@@ -821,7 +859,13 @@ int build_bvh8(const float* d_vtx, const uint32_t* d_idx, const uint32_t* d_triM
             }
         }
         WRK_BCHECK(cudaEventRecord(e1, st));
-        WRK_BCHECK(cudaEventSynchronize(e1));
+        // SAH cost of the finished tree (outside the timed build)
+        double hs[2] = {0.0, 0.0};
+        WRK_BCHECK(cudaMemsetAsync(scan, 0, 2 * sizeof(double), st));
+        if (hcc.nodes) k_sah<<<grid_for(hcc.nodes, 256), 256, 0, st>>>(onodes, hcc.nodes, (double*)scan);
+        WRK_BCHECK(cudaGetLastError());
+        WRK_BCHECK(cudaMemcpyAsync(hs, scan, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        WRK_BCHECK(cudaStreamSynchronize(st));
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
         if (hcc.tris != n) {
@@ -835,7 +879,7 @@ int build_bvh8(const float* d_vtx, const uint32_t* d_idx, const uint32_t* d_triM
         out->numBinary = numBinary;
         out->depth = hcc.maxDepth;
         out->ms = ms;
-        out->sah = 0.0f;
+        out->sah = hs[1] > 0.0 ? (float)(1.0 + hs[0] / hs[1]) : 0.0f;
         onodes = nullptr;
         otris = nullptr;
         rc = WRK_OK;
