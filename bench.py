@@ -354,7 +354,12 @@ def main():
     scene = wrk.Scene.from_data(sd, device=local)
     # launch shape (queue capacity, graph chunk, shading block) picked by the
     # project's autotuner on this workload at 1/16 of its spp
-    tune = wrk.autotune(scene, spp=max(1, st.spp // 16), device=local)
+    # (rank 0 tunes and every rank uses its choice, so the ranks run the same shape)
+    tune = wrk.autotune(scene, spp=max(1, st.spp // 16), device=local) if rank == 0 else None
+    if dist is not None:
+        box = [tune]
+        dist.broadcast_object_list(box, src=0)
+        tune = box[0]
     rend = wrk.Renderer(device=local, capacity=tune["capacity"])
     rend.set_launch(tune["chunk"], tune["shadeBlock"])
     npx = st.width * st.height
