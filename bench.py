@@ -156,15 +156,21 @@ def served_legs(args, rend, local):
     dn = wrk.Denoiser(device=local)
     meta = denoise_train.load_weights(dn)
     sd = scenes.scale_test(1920, 1080, 64, seed=1)
-    scene = wrk.Scene.from_data(sd, device=local)
+    # BVH build of the scale scene (GPU binned SAH -> 8-wide nodes), device time; the
+    # scene is uploaded three times and the fastest build is reported (the first one
+    # can meet host threads still spinning down from the CPU-baseline leg)
+    builds = []
+    for _ in range(3):
+        scene = wrk.Scene.from_data(sd, device=local)
+        builds.append(scene.bvh_info())
+    bi = min(builds, key=lambda b: b["buildMs"])
     st, cam = sd.settings, sd.camera
     out = {}
-    # BVH build of the scale scene (GPU binned SAH -> 8-wide nodes), device time
-    bi = scene.bvh_info()
     out["bvh_build"] = {"workload": "scale_test scene (fBm heightfield 1024^2 + 250 icospheres)",
                         "triangles": bi["numTriangles"], "nodes8": bi["numNodes"], "depth": bi["depth"],
-                        "build_ms": bi["buildMs"], "mtris_per_s": bi["numTriangles"] / (bi["buildMs"] / 1e3) / 1e6
-                        if bi["buildMs"] > 0 else None, "sah_cost": bi["sahCost"]}
+                        "build_ms": bi["buildMs"], "build_ms_all": [b["buildMs"] for b in builds],
+                        "mtris_per_s": bi["numTriangles"] / (bi["buildMs"] / 1e3) / 1e6 if bi["buildMs"] > 0 else None,
+                        "sah_cost": bi["sahCost"]}
     # denoiser inference at 1920x1080 (padded to 1920x1088 inside)
     img = torch.rand((1080, 1920, 3), device=f"cuda:{local}")
     o = torch.empty_like(img)
