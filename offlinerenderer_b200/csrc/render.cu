@@ -323,6 +323,7 @@ __device__ __forceinline__ bool rr(const Frame& f, PathRegs& r, bool delta) {
 struct LightSample {
     float3 toLight, le;
     float dist, d2, lpdf, cosTheta;
+    uint32_t tri;  // the sampled emissive triangle
 };
 __device__ __forceinline__ bool sample_light(const DevScene& s, PathRegs& r, const HitAttr& h, LightSample& ls) {
     float lu = rnd_dim(r.seed, r.dim++);
@@ -351,6 +352,7 @@ __device__ __forceinline__ bool sample_light(const DevScene& s, PathRegs& r, con
     ls.d2 = d2;
     ls.cosTheta = ct;
     ls.le = f3(lm.emission[0], lm.emission[1], lm.emission[2]);
+    ls.tri = tri;
     return true;
 }
 
@@ -361,6 +363,7 @@ struct ShadowOut {
     float3 o, d, c;
     float dist;
     uint32_t cont;
+    uint32_t lightTri;  // the light triangle the ray aims at
 };
 
 // Shades entry i of a bucket; the path's next state is left in r (and so for a
@@ -437,6 +440,7 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uin
                     so.d = ls.toLight;
                     so.dist = ls.dist;
                     so.c = con;
+                    so.lightTri = ls.tri;
                     shadow = true;
                 }
             }
@@ -611,12 +615,13 @@ __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k
             o.st[p] = make_uint4(r.seed, r.dim, (r.depth & 0xffffu) | (r.iter << 16), r.flags);
         }
         if (ps != kInvalidSlot) {
-            // sh_o.w: the request slot (every shadow ray starts at kShadowTmin);
+            // sh_o.w: the request slot and the light triangle (shadow_tag; every
+            // shadow ray starts at kShadowTmin);
             // sh_c.w: the continuation code | the continuing path's position << 2
             uint32_t w = so.cont;
             if (cx) w = pc == kInvalidSlot ? (uint32_t)kContDrop : kContExt | (pc << 2);
             if (so.cont == kContAccumulate) shd.rad[ps] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
-            shd.sh_o[ps] = make_float4(so.o.x, so.o.y, so.o.z, __uint_as_float(slot));
+            shd.sh_o[ps] = make_float4(so.o.x, so.o.y, so.o.z, __uint_as_float(shadow_tag(slot, so.lightTri)));
             shd.sh_d[ps] = make_float4(so.d.x, so.d.y, so.d.z, so.dist - kShadowTmin);
             shd.sh_c[ps] = make_float4(so.c.x, so.c.y, so.c.z, __uint_as_float(w));
         }
