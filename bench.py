@@ -73,7 +73,7 @@ TRACE_EXT_TRAFFIC_BYTES_PER_RAY = 148.5
 # SM issue-slot utilisation of the traversal and shading kernels (the roofline that
 # bounds them: SIMT integer / FP32 work, not HBM), smsp__issue_active from ncu --set
 # full on the 16-spp capture of the same scene.  CUDA events cannot measure it live.
-STAGE_ISSUE_ACTIVE = {"trace_extension": 0.710, "trace_shadow": 0.600, "shade_lambert": 0.566}
+STAGE_ISSUE_ACTIVE = {"trace_extension": 0.710, "trace_shadow": 0.473, "shade_lambert": 0.566}
 STAGE_BYTES = {"trace_extension": 48, "trace_shadow": 80, "shade_lambert": 160, "shade_dielectric": 160,
                "shade_ggx": 160, "shade_emissive": 160}
 
