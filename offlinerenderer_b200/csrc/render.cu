@@ -23,6 +23,7 @@
 // RNG is keyed by (pixel, sample), so the image does not depend on queue order.
 #include "wrk_internal.h"
 #include "wrk_shading.cuh"
+#include "wrk_tri.cuh"
 
 namespace wrk {
 
@@ -69,15 +70,21 @@ __global__ void k_control(Queues q) {
     uint32_t cur = c->cur ^ 1u;
     uint32_t out = cur ^ 1u;
     c->cur = cur;
-    // the Lambert continuations the last iteration placed at the front of ext[out]
+    // the Lambert continuations the last iteration placed at the front of ext[out];
+    // those whose shadow query the shade answered have no shadow entry and count
+    // as live paths here
     c->ext[out].v = c->cont.v;
     c->cont.v = 0;
+    const uint32_t direct = c->contDirect.v;
+    c->contDirect.v = 0;
+    c->shdRays += c->shadowAnswered.v;
+    c->shadowAnswered.v = 0;
     c->shd[out].v = 0;
     for (int b = 0; b < kNumBuckets; ++b) c->bucket[b].v = 0;
     c->fetchExtension.v = 0;
     c->fetchShadow.v = 0;
     // every live path holds one extension or shadow entry: the rest is room for new ones
-    uint32_t live = c->ext[cur].v + c->shd[cur].v;
+    uint32_t live = c->ext[cur].v + c->shd[cur].v + direct;
     if (c->ext[cur].v > q.capacity || c->shd[cur].v > q.capacity || live > q.capacity) {
         c->error |= kErrQueueOverflow;
         live = q.capacity;
@@ -282,7 +289,9 @@ __device__ __forceinline__ float3 normal_mapped(const DevScene& s, const wrk_mat
     return h.n;
 }
 
-enum : int { kOutNone = 0, kOutExt = 1, kOutShadow = 2, kOutDone = 3 };
+// kOutCont: a Lambert path whose shadow query was answered in the shade (its light
+// blocks the ray) and that continues: only its next extension entry is written.
+enum : int { kOutNone = 0, kOutExt = 1, kOutShadow = 2, kOutDone = 3, kOutCont = 4 };
 
 struct PathRegs {
     float3 o, d, thr, rad;
@@ -364,6 +373,7 @@ struct ShadowOut {
     float dist;
     uint32_t cont;
     uint32_t lightTri;  // the light triangle the ray aims at
+    bool answered;      // the shadow query was answered here (the light blocks the ray)
 };
 
 // Shades entry i of a bucket; the path's next state is left in r (and so for a
@@ -484,6 +494,17 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uin
                     so.cont = kContExt;
                 }
             }
+            // The shadow ray offset 1e-4 along the normal but ending 1e-5 short of
+            // the light often hits the light triangle itself: then the query's
+            // answer (occluded) is known here, the shadow kernel has nothing to do,
+            // and the path only continues, accumulates or ends.
+            const Ray sr{so.o.x, so.o.y, so.o.z, so.d.x, so.d.y, so.d.z, kShadowTmin, so.dist - kShadowTmin};
+            if (so.lightTri < s.numTris && light_blocks(s, sr, so.lightTri)) {
+                so.answered = true;
+                if (so.cont == kContExt) return kOutCont;
+                if (so.cont == kContAccumulate) accumulate(f, r);
+                return kOutDone;
+            }
             return kOutShadow;
         }
     } else if (kBucket == kBucketDielectric) {
@@ -583,6 +604,7 @@ __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k
         PathRegs r;
         ShadowOut so;
         so.cont = kContDrop;
+        so.answered = false;
         int out = kOutNone;
         uint32_t slot = 0;
         if (i < n) {
@@ -603,8 +625,18 @@ __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k
         // extension buffer it will be traced from two iterations on (this
         // iteration's input, no longer read); the control kernel of the next
         // iteration starts that queue after these entries.
-        const bool cx = ps != kInvalidSlot && so.cont == kContExt;
+        const bool cx = (ps != kInvalidSlot && so.cont == kContExt) || out == kOutCont;
         const uint32_t pc = append_pos(&c->cont.v, cx, q.capacity, &c->error);
+        // shadow queries answered here: counted as traced, and the continuations
+        // they leave (no shadow entry) held as live paths until traced
+        {
+            const uint32_t ans = __ballot_sync(0xffffffffu, so.answered);
+            const uint32_t direct = __ballot_sync(0xffffffffu, out == kOutCont && pc != kInvalidSlot);
+            if ((threadIdx.x & 31u) == 0) {
+                if (ans) atomicAdd(&c->shadowAnswered.v, (uint32_t)__popc(ans));
+                if (direct) atomicAdd(&c->contDirect.v, (uint32_t)__popc(direct));
+            }
+        }
         if (pe != kInvalidSlot || pc != kInvalidSlot) {
             const PathQ o = pe != kInvalidSlot ? ext : (cur ? q.ext[1] : q.ext[0]);
             const uint32_t p = pe != kInvalidSlot ? pe : pc;
@@ -615,13 +647,12 @@ __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k
             o.st[p] = make_uint4(r.seed, r.dim, (r.depth & 0xffffu) | (r.iter << 16), r.flags);
         }
         if (ps != kInvalidSlot) {
-            // sh_o.w: the request slot and the light triangle (shadow_tag; every
-            // shadow ray starts at kShadowTmin);
+            // sh_o.w: the request slot (every shadow ray starts at kShadowTmin);
             // sh_c.w: the continuation code | the continuing path's position << 2
             uint32_t w = so.cont;
             if (cx) w = pc == kInvalidSlot ? (uint32_t)kContDrop : kContExt | (pc << 2);
             if (so.cont == kContAccumulate) shd.rad[ps] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
-            shd.sh_o[ps] = make_float4(so.o.x, so.o.y, so.o.z, __uint_as_float(shadow_tag(slot, so.lightTri)));
+            shd.sh_o[ps] = make_float4(so.o.x, so.o.y, so.o.z, __uint_as_float(slot));
             shd.sh_d[ps] = make_float4(so.d.x, so.d.y, so.d.z, so.dist - kShadowTmin);
             shd.sh_c[ps] = make_float4(so.c.x, so.c.y, so.c.z, __uint_as_float(w));
         }

@@ -17,6 +17,7 @@
 // oracle's.
 #include "wrk_internal.h"
 #include "wrk_shading.cuh"
+#include "wrk_tri.cuh"
 
 namespace wrk {
 
@@ -24,49 +25,6 @@ constexpr int kTraceBlock = 128;
 constexpr int kStackSmem = 12;
 constexpr int kStackLocal = 36;
 constexpr uint32_t kMaxVisits = 1u << 16;
-
-struct Ray {
-    float ox, oy, oz, dx, dy, dz, tmin, tmax;
-};
-
-// Moller-Trumbore without the reciprocal: barycentric numerators are compared
-// with det (sign-aware) and t is divided only for hits inside the triangle.  Each
-// cross-product component is one product and one FMA, each dot product one product
-// and two FMAs (correctly rounded intrinsics, in the CPU oracle's exact order).
-__device__ __forceinline__ bool mt_rn(const Ray& r, float4 a, float4 b, float4 c, float& t) {
-    float px = __fmaf_rn(r.dy, c.z, -__fmul_rn(r.dz, c.y));
-    float py = __fmaf_rn(r.dz, c.x, -__fmul_rn(r.dx, c.z));
-    float pz = __fmaf_rn(r.dx, c.y, -__fmul_rn(r.dy, c.x));
-    float det = __fmaf_rn(b.x, px, __fmaf_rn(b.y, py, __fmul_rn(b.z, pz)));
-    float sx = __fsub_rn(r.ox, a.x), sy = __fsub_rn(r.oy, a.y), sz = __fsub_rn(r.oz, a.z);
-    float un = __fmaf_rn(sx, px, __fmaf_rn(sy, py, __fmul_rn(sz, pz)));
-    float qx = __fmaf_rn(sy, b.z, -__fmul_rn(sz, b.y));
-    float qy = __fmaf_rn(sz, b.x, -__fmul_rn(sx, b.z));
-    float qz = __fmaf_rn(sx, b.y, -__fmul_rn(sy, b.x));
-    float vn = __fmaf_rn(r.dx, qx, __fmaf_rn(r.dy, qy, __fmul_rn(r.dz, qz)));
-    float uv = __fadd_rn(un, vn);
-    bool inside = det > 0.0f ? (un >= 0.0f && vn >= 0.0f && uv <= det)
-                             : (det < 0.0f && un <= 0.0f && vn <= 0.0f && uv >= det);
-    if (!inside) return false;
-    t = __fdiv_rn(__fmaf_rn(c.x, qx, __fmaf_rn(c.y, qy, __fmul_rn(c.z, qz))), det);
-    return true;
-}
-
-// Does the ray hit scene triangle `prim` within [tmin, tmax]?  The triangle record
-// is rebuilt from the scene's vertices exactly as the BVH builder writes it (v0,
-// v1 - v0, v2 - v0 with correctly rounded subtractions), so the answer is the one
-// the traversal's triangle test gives for the same triangle.
-__device__ __forceinline__ bool light_blocks(const DevScene& s, const Ray& r, uint32_t prim) {
-    const uint32_t i0 = __ldg(s.idx + 3 * prim), i1 = __ldg(s.idx + 3 * prim + 1), i2 = __ldg(s.idx + 3 * prim + 2);
-    const float ax = __ldg(s.vtx + 3 * i0), ay = __ldg(s.vtx + 3 * i0 + 1), az = __ldg(s.vtx + 3 * i0 + 2);
-    const float bx = __ldg(s.vtx + 3 * i1), by = __ldg(s.vtx + 3 * i1 + 1), bz = __ldg(s.vtx + 3 * i1 + 2);
-    const float cx = __ldg(s.vtx + 3 * i2), cy = __ldg(s.vtx + 3 * i2 + 1), cz = __ldg(s.vtx + 3 * i2 + 2);
-    const float4 a = make_float4(ax, ay, az, 0.0f);
-    const float4 b = make_float4(__fsub_rn(bx, ax), __fsub_rn(by, ay), __fsub_rn(bz, az), 0.0f);
-    const float4 c = make_float4(__fsub_rn(cx, ax), __fsub_rn(cy, ay), __fsub_rn(cz, az), 0.0f);
-    float th;
-    return mt_rn(r, a, b, c, th) && th >= r.tmin && th <= r.tmax;
-}
 
 // Byte k of w as the float 2^15 + b, exactly, without an int->float conversion:
 // one byte permute builds the bits 0x4700bb00 (exponent 2^15, b in mantissa bits
@@ -419,10 +377,8 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
                 if (idx < n) {
                     float4 o = kAnyHit ? in.sh_o[idx] : in.ray_o[idx];
                     float4 d = kAnyHit ? in.sh_d[idx] : in.ray_d[idx];
-                    // a shadow entry keeps its request slot and light triangle where
-                    // tmin would be
-                    const uint32_t tag = __float_as_uint(o.w);
-                    const uint32_t slot = kAnyHit ? (tag & 0xffu) : slot_of(in.st[idx].w);
+                    // a shadow entry keeps its request slot where tmin would be
+                    const uint32_t slot = kAnyHit ? __float_as_uint(o.w) : slot_of(in.st[idx].w);
                     if (kAnyHit) o.w = kShadowTmin;
                     if constexpr (kMulti) {
                         sceneIdx = q.req[slot].scene;
@@ -430,19 +386,6 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
                         geo = TraceGeom{sc.nodes, sc.tris, sc.numNodes, sc.numTris};
                     }
                     trav_init(t, Ray{o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w});
-                    if (kAnyHit) {
-                        // Test the light triangle the ray aims at first: a shadow ray
-                        // that stops short of the light by less than its origin offset
-                        // hits the light itself, and any hit in [tmin, tmax] answers
-                        // the query (the traversal would find this one or another), so
-                        // the ray is done without visiting a node.
-                        const uint32_t lt = tag >> 8;
-                        const DevScene& sc = kMulti ? q.scenes[sceneIdx] : s0;
-                        if (lt < sc.numTris && light_blocks(sc, t.r, lt)) {
-                            t.pBest = lt;
-                            t.gHits = 0;  // nothing left to traverse: the first step ends the ray
-                        }
-                    }
                     active = true;
                 } else {
                     exhausted = true;
@@ -468,7 +411,7 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
                 const uint32_t w = __float_as_uint(cc.w);
                 const bool lit = t.pBest == kNoHit;
                 cont = w & 3u;
-                slot = __float_as_uint(in.sh_o[idx].w) & 0xffu;
+                slot = __float_as_uint(in.sh_o[idx].w);
                 if (cont == kContExt) {
                     // the continuing path's entry waits in the next extension queue
                     const uint32_t pos = w >> 2;

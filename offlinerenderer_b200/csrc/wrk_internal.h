@@ -54,12 +54,7 @@ enum : uint32_t { kContExt = 0u, kContAccumulate = 1u, kContDrop = 2u };
 // Start of every shadow ray's [tmin, tmax] (the light sample's distance minus it
 // is tmax), so the queue does not store it.
 constexpr float kShadowTmin = 1e-5f;
-// sh_o.w of a shadow entry: the request slot in bits 0-7 and the light triangle the
-// ray aims at in bits 8-31 (all ones: not recorded, triangle index >= 2^24 - 1).
-constexpr uint32_t kNoLightTri = 0xffffffu;
-__host__ __device__ inline uint32_t shadow_tag(uint32_t slot, uint32_t lightTri) {
-    return (slot & 0xffu) | ((lightTri < kNoLightTri ? lightTri : kNoLightTri) << 8);
-}
+
 constexpr uint32_t kSlotShift = 8;
 __host__ __device__ inline uint32_t slot_of(uint32_t stw) { return (stw >> kSlotShift) & 0xffu; }
 
@@ -132,6 +127,8 @@ struct Counters {
     HotCounter shd[2];
     HotCounter bucket[kNumBuckets];
     HotCounter cont;            // Lambert continuations placed in ext[cur] this iteration
+    HotCounter contDirect;      // ... of them without a shadow entry (query answered in the shade)
+    HotCounter shadowAnswered;  // shadow queries the Lambert shade answered this iteration
     HotCounter fetchExtension;  // rays taken by the persistent traversal kernels this iteration
     HotCounter fetchShadow;
     uint32_t cur;          // which ext/shd buffer the current iteration consumes
