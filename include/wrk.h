@@ -94,7 +94,8 @@ enum {
 typedef struct {
     uint64_t paths;          /* camera paths started */
     uint64_t extensionRays;  /* closest-hit rays traced */
-    uint64_t shadowRays;     /* any-hit rays traced */
+    uint64_t shadowRays;     /* any-hit (shadow) queries answered, by traversal or by the
+                                light-triangle test of the Lambert shade */
     uint32_t iterations;     /* wavefront iterations issued */
     uint32_t deviceErrors;   /* internal device error flags raised (0 = none) */
     float gpuMs;             /* device time of the render loop (CUDA events) */
