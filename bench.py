@@ -250,6 +250,20 @@ def batched_scenes_leg(local):
             "autotune": {k: tune[k] for k in ("capacity", "chunk", "shadeBlock", "bestMs")}}
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (first processor in /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or "unknown"
+
+
 def cpu_reference_rate(sd, threads: int, target_s: float = 12.0):
     """Reference shading code on the host cores (oracle/_ref), bounded sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -273,6 +287,7 @@ def cpu_reference_rate(sd, threads: int, target_s: float = 12.0):
     dt = time.perf_counter() - t0
     samples = st.width * st.height * spp
     return {"value": samples / dt / 1e6, "unit": "Msamples/s", "cores": threads, "kind": kind,
+            "cpu_model": cpu_model(),
             "sample": f"{st.width}x{st.height} at {spp} spp of the same scene and settings ({samples} samples, "
                       f"{dt:.1f} s)",
             "mrays_per_s": (s2["extension_rays"] + s2["shadow_rays"]) / dt / 1e6}
@@ -310,7 +325,7 @@ def run_reference_arm(args, cfg):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
            "config": {"workload": cfg["workload"], "step": f"{st.width}x{st.height} at 1 spp on the host cores"},
-           "cpu_baseline": {"value": v, "unit": "Msamples/s", "cores": threads, "kind": kind,
+           "cpu_baseline": {"value": v, "unit": "Msamples/s", "cores": threads, "kind": kind, "cpu_model": cpu_model(),
                             "sample": f"{args.steps} steps of {st.width}x{st.height} at 1 spp"},
            "e2e": {"value": v, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
            "mrays_per_s": rays / dt / 1e6}
@@ -391,11 +406,13 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     iters = 0
-    rays = 0
+    rays = 0          # rays traversed: extension + traced shadow rays
+    queries = 0       # + the shadow queries the Lambert shade answered without a traversal
     for i in range(args.steps):
         s = step(args.warmup + i)
         iters += s["iterations"]
-        rays += s["extensionRays"] + s["shadowRays"]
+        rays += s["extensionRays"] + s["shadowTraced"]
+        queries += s["extensionRays"] + s["shadowRays"]
     e1.record()
     torch.cuda.synchronize()
     if dist is not None:
@@ -408,11 +425,12 @@ def main():
         ms = float(t.item())
     value = world * args.steps * samples_per_step / (ms / 1e3) / 1e6
     mrays = world * rays / (ms / 1e3) / 1e6
+    mqueries = world * queries / (ms / 1e3) / 1e6
 
     # per-stage device times (events on the renderer's stream), one extra render
     tst = rend.render_device(scene, None, d_rgb_ptr=wrk.TensorPtr(frame).ptr, stage_timing=True)
     stage_ms = tst["stageMs"]
-    units = {"trace_extension": tst["extensionRays"], "trace_shadow": tst["shadowRays"],
+    units = {"trace_extension": tst["extensionRays"], "trace_shadow": tst["shadowTraced"],
              "shade_lambert": tst["bucketPaths"]["lambert"], "shade_dielectric": tst["bucketPaths"]["dielectric"],
              "shade_ggx": tst["bucketPaths"]["ggx"], "shade_emissive": tst["bucketPaths"]["other"]}
     dominant = max(STAGE_BYTES, key=lambda k: stage_ms[k])
@@ -471,6 +489,10 @@ def main():
                        "l2": f"per-step working set exceeds the 126 MB L2 (path queues: {tune['capacity']} entries "
                              f"x 672 B = {tune['capacity'] * 672 / 1e9:.1f} GB)"},
             "mrays_per_s": mrays,
+            "mrays_per_s_note": "extension rays + shadow rays traversed by the any-hit kernel",
+            "mrays_per_s_incl_answered": mqueries,
+            "shadow_queries_per_step": {"traced": tst["shadowTraced"],
+                                        "answered_in_shade": tst["shadowRays"] - tst["shadowTraced"]},
             "iterations_per_step": iters / args.steps,
             "gpu_launches": iters * 9 + args.steps * 2,
             "e2e": {"value": e2e_val, "unit": "Msamples/s", "h2d_bytes_per_step": 76 + 44,

@@ -7,8 +7,7 @@
 #include <string>
 
 #include "wr/types.h"
-
-struct wrk_scene;
+#include "wrk.h"
 
 namespace wr {
 
@@ -38,13 +37,28 @@ public:
     explicit Scene(int deviceId);
     ~Scene();
 
-    // Material creation (returns the material id)
-    uint32_t addLambertianMaterial(const Vec3& albedo);
-    uint32_t addLambertianMaterial(const Vec3& albedo, uint32_t albedoTextureId);
-    uint32_t addEmissiveMaterial(const Vec3& emission);
-    uint32_t addGlassMaterial(const Vec3& albedo, float ior);
-    uint32_t addGGXReflectionMaterial(const Vec3& albedo, float roughness, float metallic = 0.0f);
-    uint32_t addGGXTransmissionMaterial(const Vec3& albedo, float roughness, float ior);
+    // Material creation (returns the material id), with libWR's defaults for the
+    // fields a material type does not take (scene.cpp:91-168).
+    uint32_t addLambertianMaterial(const Vec3& albedo) { return addLambertianMaterial(albedo, 0u); }
+    uint32_t addLambertianMaterial(const Vec3& albedo, uint32_t albedoTextureId) {
+        return addMaterialRecord(material(WRK_LAMBERTIAN, albedo.x, albedo.y, albedo.z, 0.0f, 0.0f, 0.0f, 1.0f, 1.0f,
+                                          0.0f, albedoTextureId));
+    }
+    uint32_t addEmissiveMaterial(const Vec3& emission) {
+        return addMaterialRecord(
+            material(WRK_EMISSIVE, 0.0f, 0.0f, 0.0f, emission.x, emission.y, emission.z, 1.0f, 0.0f, 0.0f, 0u));
+    }
+    uint32_t addGlassMaterial(const Vec3& albedo, float ior) {
+        return addMaterialRecord(material(WRK_GLASS, albedo.x, albedo.y, albedo.z, 0.0f, 0.0f, 0.0f, ior, 0.0f, 0.0f, 0u));
+    }
+    uint32_t addGGXReflectionMaterial(const Vec3& albedo, float roughness, float metallic = 0.0f) {
+        return addMaterialRecord(material(WRK_GGX_REFLECTION, albedo.x, albedo.y, albedo.z, 0.0f, 0.0f, 0.0f, 1.5f,
+                                          roughness, metallic, 0u));
+    }
+    uint32_t addGGXTransmissionMaterial(const Vec3& albedo, float roughness, float ior) {
+        return addMaterialRecord(material(WRK_GGX_TRANSMISSION, albedo.x, albedo.y, albedo.z, 0.0f, 0.0f, 0.0f, ior,
+                                          roughness, 0.0f, 0u));
+    }
 
     void setMaterialNormalMap(uint32_t materialId, uint32_t normalTextureId);
 
@@ -55,7 +69,7 @@ public:
     void addTriangleMesh(std::span<const float> vertices, std::span<const uint32_t> indices,
                          std::span<const float> normals, std::span<const float> uvs, uint32_t materialId);
 
-    void setEnvironmentRadiance(const Vec3& radiance);
+    void setEnvironmentRadiance(const Vec3& radiance) { setEnvironmentRadianceRGB(radiance.x, radiance.y, radiance.z); }
     // Loads a Radiance .hdr map; stored with the scene.  libWR's miss program
     // shades with the uniform radiance only (trace.cu:143-148), and so does this.
     void setEnvironmentMap(const std::string& hdrPath);
@@ -70,7 +84,11 @@ public:
     DevicePtr getMaterialsBuffer() const;
     TraversableHandle getGASHandle() const;  // the BVH node array
     uint32_t getNumMaterials() const;
-    Vec3 getEnvironmentRadiance() const;
+    Vec3 getEnvironmentRadiance() const {
+        float c[3];
+        environmentRadianceRGB(c);
+        return Vec3(c[0], c[1], c[2]);
+    }
     uint64_t getEnvironmentMapTexture() const;
     uint32_t getEnvironmentMapWidth() const;
     uint32_t getEnvironmentMapHeight() const;
@@ -88,6 +106,28 @@ public:
     uint32_t addTexture(const uint8_t* rgba, uint32_t width, uint32_t height);
     // Additive: the C-ABI handle (valid after finalize).
     wrk_scene* native() const;
+
+    // Additive: the Vec3-free forms the inline members above call.  libwrk.so
+    // exports only these, so its symbols do not depend on the caller's Vec3.
+    uint32_t addMaterialRecord(const wrk_material& m);
+    void setEnvironmentRadianceRGB(float r, float g, float b);
+    void environmentRadianceRGB(float rgb[3]) const;
+    static wrk_material material(uint32_t type, float ar, float ag, float ab, float er, float eg, float eb, float ior,
+                                 float roughness, float metallic, uint32_t albedoTextureId) {
+        wrk_material m{};
+        m.albedo[0] = ar;
+        m.albedo[1] = ag;
+        m.albedo[2] = ab;
+        m.emission[0] = er;
+        m.emission[1] = eg;
+        m.emission[2] = eb;
+        m.ior = ior;
+        m.type = type;
+        m.roughness = roughness;
+        m.metallic = metallic;
+        m.albedoTextureId = albedoTextureId;
+        return m;
+    }
 
 private:
     SceneImpl* m_impl;

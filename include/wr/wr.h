@@ -1,11 +1,11 @@
-// Umbrella header of the drop-in C++ API (libWR/include/wr/wr.h).
+// Umbrella header of the drop-in C++ API (libWR/include/wr/wr.h): the same four
+// headers.  The test-layer image writers are in wr/image.h, included separately.
 #pragma once
 
-#include "wr/context.h"
-#include "wr/image.h"
-#include "wr/renderer.h"
-#include "wr/scene.h"
 #include "wr/types.h"
+#include "wr/context.h"
+#include "wr/scene.h"
+#include "wr/renderer.h"
 
 namespace wr {
 

@@ -104,6 +104,8 @@ typedef struct {
     uint32_t stageLaunches[9];
     uint64_t bucketPaths[5]; /* paths shaded per bucket: Lambert, dielectric, GGX, emissive/other, and the
                                 Lambert paths the shadow stage continued after their shadow ray */
+    uint64_t shadowTraced;   /* the part of shadowRays the any-hit kernel traced (the rest were
+                                answered by the Lambert shade's light-triangle test) */
 } wrk_render_stats;
 
 typedef struct {
@@ -265,8 +267,11 @@ int wrk_compact(const uint32_t* d_stage, const uint32_t* d_idxIn, uint32_t n, ui
  * that must own all device memory): the per-tile counts live in a 256 KiB array
  * built into the library, so n is limited to 67,108,864 indices (larger n returns
  * WRK_ERR_INVALID).  The first call on a device resolves that array's address and
- * should come before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race and must be serialized by the caller. */
+ * should come before any stream capture; the address is kept for the life of the
+ * process, so a cudaDeviceReset of that device after the first call, or a
+ * non-primary driver context made current on it, is not supported.  All calls
+ * share the array: calls that overlap on the GPU race and must be serialized by
+ * the caller. */
 int wrk_compact_noalloc(const uint32_t* d_stage, const uint32_t* d_idxIn, uint32_t n, uint32_t* d_idxOut,
                         uint32_t* d_count);
 /* Light selection (sampleEmissiveTriangle, sampling.cuh:116-135). */

@@ -29,7 +29,10 @@ CPP_SOURCES = ["wr_api.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off",
                      "-I", INCLUDE, "-diag-suppress", "550"]
-CXX_FLAGS = ["-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", "-I", INCLUDE, "-I", os.path.join(CUDA_HOME, "include")]
+# -fvisibility-inlines-hidden: the inline members of include/wr/*.h (the ones that
+# take a Vec3) are compiled into the caller, never exported from libwrk.so.
+CXX_FLAGS = ["-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", "-fvisibility-inlines-hidden", "-I", INCLUDE,
+             "-I", os.path.join(CUDA_HOME, "include")]
 
 
 def _headers():

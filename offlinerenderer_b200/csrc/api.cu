@@ -784,6 +784,7 @@ static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, con
         stats->paths = h.paths;
         stats->extensionRays = h.extRays;
         stats->shadowRays = h.shdRays + h.shadowAnswered.v;  // + the last iteration's answered queries
+        stats->shadowTraced = h.shdTraced;
         for (int b = 0; b < kNumBuckets; ++b) stats->bucketPaths[b] = h.bucketTotal[b] + h.bucket[b].v;
         stats->iterations = iters;
         stats->deviceErrors = h.error;

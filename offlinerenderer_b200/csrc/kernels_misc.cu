@@ -90,7 +90,8 @@ __global__ void k_compact_write(const uint32_t* __restrict__ stage, const uint32
 
 int compact_stable(const uint32_t* stage, const uint32_t* idx, uint32_t n, uint32_t* out, uint32_t* count,
                    cudaStream_t st) {
-    uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
+    // in 64 bits: n + 1023 wraps for n > 2^32 - 1024 (at most 4,194,304 tiles fit a grid)
+    const uint32_t tiles = (uint32_t)(((uint64_t)n + kCompactTile - 1) / kCompactTile);
     if (tiles == 0) return cudaMemsetAsync(count, 0, sizeof(uint32_t), st) == cudaSuccess ? WRK_OK : WRK_ERR_CUDA;
     uint32_t* tileCount = nullptr;
     if (cudaMallocAsync(&tileCount, sizeof(uint32_t) * tiles, st) != cudaSuccess) return WRK_ERR_CUDA;
@@ -236,12 +237,15 @@ void launch_tonemap(const float* rgb, uint32_t nfloat, uint8_t* out, int grid, i
 // allocator has to own every device byte, and hosts that forbid allocation after
 // start-up so that memory use stays fixed.  For them wrk_compact_noalloc keeps
 // that scratch in a fixed array that is part of the library image itself (loaded
-// with the module, resident on every GPU that loads the library until the
-// process exits), so the call allocates nothing.
+// with the module into each device's primary context, and held there until the
+// process exits or that context is reset), so the call allocates nothing.
 //
 // The first call on each device resolves the array's device address (with
 // cudaGetSymbolAddress, that device current); make that first call before any
-// stream capture begins.
+// stream capture begins.  The address is kept for the life of the process, so
+// this entry point supports neither a cudaDeviceReset of that device after its
+// first call (the module is reloaded elsewhere and the kept address dangles) nor
+// a caller that makes a non-primary driver context current on the device.
 //
 // Limit: at most kNoAllocMaxTiles tiles of 1024 entries (67,108,864 input
 // indices), i.e. 256 KiB of scratch per GPU.  Every call shares this one array
@@ -286,11 +290,13 @@ extern "C" int wrk_compact_noalloc(const uint32_t* d_stage, const uint32_t* d_id
     using namespace wrk;
     if (!d_count || (n && (!d_stage || !d_idxIn || !d_idxOut)))
         return report_error(WRK_ERR_INVALID, "wrk_compact_noalloc: null buffer");
-    const uint32_t tiles = (n + kCompactTile - 1) / kCompactTile;
-    if (tiles > kNoAllocMaxTiles)
+    // in 64 bits, so that n close to 2^32 cannot wrap to zero tiles and pass the limit
+    const uint64_t tiles64 = ((uint64_t)n + kCompactTile - 1) / kCompactTile;
+    if (tiles64 > kNoAllocMaxTiles)
         return report_error(WRK_ERR_INVALID,
                             "wrk_compact_noalloc: n exceeds the fixed scratch limit of 67108864 indices "
                             "(65536 tiles of 1024); use wrk_compact");
+    const uint32_t tiles = (uint32_t)tiles64;
     uint32_t* scratch = nullptr;
     int rc = scratch_for_current_device(&scratch);
     if (rc) return rc;

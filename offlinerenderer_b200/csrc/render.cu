@@ -121,6 +121,7 @@ __global__ void k_control(Queues q) {
     c->paths += g;
     c->extRays += c->ext[cur].v;
     c->shdRays += c->shd[cur].v;
+    c->shdTraced += c->shd[cur].v;
     c->iteration += 1;
 }
 

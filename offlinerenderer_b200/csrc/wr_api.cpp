@@ -7,6 +7,10 @@
 // libwrk, which builds the light CDF and the BVH on the GPU.  Failures of the C
 // ABI are rethrown as std::runtime_error, libWR's error convention
 // (libWR/src/internal/cuda_utils.h:13-39).
+//
+// Only the members without a Vec3 / Camera / RenderParams in their signature are
+// defined here; the others are inline in include/wr/*.h and call these, so the
+// library serves callers whose wr::Vec3 is glm::vec3 as well as the GLM-free one.
 #include <zlib.h>
 
 #include <algorithm>
@@ -21,7 +25,6 @@
 #include <string>
 #include <vector>
 
-#include "../../include/wr/image.h"
 #include "../../include/wr/wr.h"
 #include "../../include/wrk.h"
 
@@ -193,7 +196,7 @@ struct SceneImpl {
     std::vector<uint32_t> texW, texH;
     std::vector<float> envMap;
     uint32_t envW = 0, envH = 0;
-    Vec3 env{0, 0, 0};
+    float env[3] = {0.0f, 0.0f, 0.0f};
     bool hasNormals = false, hasUVs = false, finalized = false;
     wrk_scene* handle = nullptr;
     wrk_scene_buffers bufs{};
@@ -206,43 +209,13 @@ struct SceneImpl {
     }
 };
 
-static wrk_material make_material(uint32_t type, const Vec3& albedo, const Vec3& emission, float ior, float rough,
-                                  float metal, uint32_t tex) {
-    wrk_material m{};
-    m.albedo[0] = albedo.x;
-    m.albedo[1] = albedo.y;
-    m.albedo[2] = albedo.z;
-    m.emission[0] = emission.x;
-    m.emission[1] = emission.y;
-    m.emission[2] = emission.z;
-    m.ior = ior;
-    m.type = type;
-    m.roughness = rough;
-    m.metallic = metal;
-    m.albedoTextureId = tex;
-    return m;
-}
-
 Scene::Scene() : m_impl(new SceneImpl()) {}
 Scene::Scene(int deviceId) : m_impl(new SceneImpl()) { m_impl->device = deviceId; }
 Scene::~Scene() { delete m_impl; }
 
-// Material defaults as libWR's Scene (scene.cpp:91-168).
-uint32_t Scene::addLambertianMaterial(const Vec3& albedo) { return addLambertianMaterial(albedo, 0); }
-uint32_t Scene::addLambertianMaterial(const Vec3& albedo, uint32_t tex) {
-    return m_impl->add(make_material(WRK_LAMBERTIAN, albedo, Vec3(0, 0, 0), 1.0f, 1.0f, 0.0f, tex));
-}
-uint32_t Scene::addEmissiveMaterial(const Vec3& emission) {
-    return m_impl->add(make_material(WRK_EMISSIVE, Vec3(0, 0, 0), emission, 1.0f, 0.0f, 0.0f, 0));
-}
-uint32_t Scene::addGlassMaterial(const Vec3& albedo, float ior) {
-    return m_impl->add(make_material(WRK_GLASS, albedo, Vec3(0, 0, 0), ior, 0.0f, 0.0f, 0));
-}
-uint32_t Scene::addGGXReflectionMaterial(const Vec3& albedo, float roughness, float metallic) {
-    return m_impl->add(make_material(WRK_GGX_REFLECTION, albedo, Vec3(0, 0, 0), 1.5f, roughness, metallic, 0));
-}
-uint32_t Scene::addGGXTransmissionMaterial(const Vec3& albedo, float roughness, float ior) {
-    return m_impl->add(make_material(WRK_GGX_TRANSMISSION, albedo, Vec3(0, 0, 0), ior, roughness, 0.0f, 0));
+uint32_t Scene::addMaterialRecord(const wrk_material& m) {
+    if (m_impl->finalized) throw std::runtime_error("Scene already finalized");
+    return m_impl->add(m);
 }
 void Scene::setMaterialNormalMap(uint32_t materialId, uint32_t normalTextureId) {
     if (materialId >= m_impl->materials.size()) throw std::runtime_error("Invalid material ID");
@@ -282,7 +255,14 @@ void Scene::addTriangleMesh(std::span<const float> v, std::span<const uint32_t> 
     s.triMat.insert(s.triMat.end(), nt, mat);
 }
 
-void Scene::setEnvironmentRadiance(const Vec3& r) { m_impl->env = r; }
+void Scene::setEnvironmentRadianceRGB(float r, float g, float b) {
+    m_impl->env[0] = r;
+    m_impl->env[1] = g;
+    m_impl->env[2] = b;
+}
+void Scene::environmentRadianceRGB(float rgb[3]) const {
+    for (int k = 0; k < 3; ++k) rgb[k] = m_impl->env[k];
+}
 void Scene::setEnvironmentMap(const std::string& path) {
     decode_hdr(read_file(path), m_impl->envMap, m_impl->envW, m_impl->envH);
 }
@@ -332,8 +312,7 @@ void Scene::finalize(const SceneBuildConfig&) {
                                     gone ? 1 : s.texH[i], &id),
               "wrk_scene_add_texture");
     }
-    float env[3] = {s.env.x, s.env.y, s.env.z};
-    check(wrk_scene_set_environment(s.handle, env), "wrk_scene_set_environment");
+    check(wrk_scene_set_environment(s.handle, s.env), "wrk_scene_set_environment");
     if (!s.envMap.empty())
         check(wrk_scene_set_environment_map(s.handle, s.envMap.data(), s.envW, s.envH),
               "wrk_scene_set_environment_map");
@@ -349,7 +328,6 @@ DevicePtr Scene::getTriangleMaterialIdsBuffer() const { return m_impl->bufs.triM
 DevicePtr Scene::getMaterialsBuffer() const { return m_impl->bufs.materials; }
 TraversableHandle Scene::getGASHandle() const { return m_impl->bufs.bvhNodes; }
 uint32_t Scene::getNumMaterials() const { return (uint32_t)m_impl->materials.size(); }
-Vec3 Scene::getEnvironmentRadiance() const { return m_impl->env; }
 uint64_t Scene::getEnvironmentMapTexture() const { return 0; }
 uint32_t Scene::getEnvironmentMapWidth() const { return m_impl->envW; }
 uint32_t Scene::getEnvironmentMapHeight() const { return m_impl->envH; }
@@ -403,43 +381,23 @@ Renderer::Renderer(const RendererConfig& config, int deviceId) : m_impl(new Rend
 Renderer::~Renderer() { delete m_impl; }
 const RenderStats& Renderer::lastStats() const { return m_impl->stats; }
 
-void Renderer::render(Scene* scene, const Camera& camera, Vec3* out, const RenderParams& p) {
+void Renderer::renderNative(Scene* scene, const wrk_camera& c, const wrk_render_params& rp, float* out,
+                            float* albedoOut, float* normalOut, bool denoise, const char* weightsPath) {
     if (!scene || !out) throw std::runtime_error("render: null scene or output buffer");
     scene->finalize();
-    wrk_camera c{};
-    c.position[0] = camera.position.x; c.position[1] = camera.position.y; c.position[2] = camera.position.z;
-    c.target[0] = camera.target.x; c.target[1] = camera.target.y; c.target[2] = camera.target.z;
-    c.up[0] = camera.up.x; c.up[1] = camera.up.y; c.up[2] = camera.up.z;
-    c.fovY = camera.fovY;
-    c.aspect = camera.aspect;
-    c.focalDistance = camera.focalDistance;
-    c.lensRadius = camera.lensRadius;
-    wrk_render_params rp{};
-    rp.width = p.width;
-    rp.height = p.height;
-    rp.spp = p.spp;
-    rp.useNEE = p.useNEE ? 1u : 0u;
-    rp.maxBounces = p.maxBounces;
-    rp.russianRouletteDepth = p.russianRouletteDepth;
-    rp.fireflyClamp = p.fireflyClamp;
-    rp.seed = p.seed;
-    rp.maxIterations = p.maxIterations;
-    rp.flags = (p.rawGuides ? WRK_FLAG_RAW_GUIDES : 0u) | (p.useEnvironmentMap ? WRK_FLAG_ENV_MAP : 0u);
     wrk_render_stats st{};
-    if (!p.denoiser.enabled) {
-        check(wrk_render(m_impl->handle, scene->native(), &c, &rp, reinterpret_cast<float*>(out),
-                         reinterpret_cast<float*>(p.albedoOut), reinterpret_cast<float*>(p.normalOut), &st),
-              "wrk_render");
+    if (!denoise) {
+        check(wrk_render(m_impl->handle, scene->native(), &c, &rp, out, albedoOut, normalOut, &st), "wrk_render");
     } else {
         // libWR denoises inside render (renderer.cpp:289-313, denoiser.cpp:17-195): render
         // rgb + averaged guides into device memory, denoise, copy the result out.
-        const std::string path = p.denoiser.weightsPath ? p.denoiser.weightsPath : default_weights();
+        const std::string path = weightsPath ? weightsPath : default_weights();
         if (!m_impl->denoiser) check(wrk_denoiser_create(m_impl->device, 1, &m_impl->denoiser), "wrk_denoiser_create");
         if (m_impl->weights != path) {
             check(wrk_denoiser_load(m_impl->denoiser, path.c_str()), "wrk_denoiser_load");
             m_impl->weights = path;
         }
-        const size_t np = (size_t)p.width * p.height, bytes = np * 12 * sizeof(float);
+        const size_t np = (size_t)rp.width * rp.height, bytes = np * 12 * sizeof(float);
         if (m_impl->dbufBytes < bytes) {
             if (m_impl->dbuf) wrk_free(m_impl->dbuf);
             m_impl->dbuf = nullptr;
@@ -452,37 +410,25 @@ void Renderer::render(Scene* scene, const Camera& camera, Vec3* out, const Rende
         dp.flags &= ~WRK_FLAG_RAW_GUIDES;  // the network takes guides averaged over spp
         check(wrk_render_device(m_impl->handle, scene->native(), &c, &dp, d, d + 3 * np, d + 6 * np, &st),
               "wrk_render_device");
-        check(wrk_denoiser_infer(m_impl->denoiser, d, d + 3 * np, d + 6 * np, 1, p.height, p.width, d + 9 * np),
+        check(wrk_denoiser_infer(m_impl->denoiser, d, d + 3 * np, d + 6 * np, 1, rp.height, rp.width, d + 9 * np),
               "wrk_denoiser_infer");
         check(wrk_memcpy_dtoh(out, d + 9 * np, np * 3 * sizeof(float)), "wrk_memcpy_dtoh");
-        const float g = p.rawGuides ? (float)p.spp : 1.0f;
-        Vec3* guides[2] = {p.albedoOut, p.normalOut};
+        const float g = (rp.flags & WRK_FLAG_RAW_GUIDES) ? (float)rp.spp : 1.0f;
+        float* guides[2] = {albedoOut, normalOut};
         for (int k = 0; k < 2; ++k) {
             if (!guides[k]) continue;
             check(wrk_memcpy_dtoh(guides[k], d + 3 * (k + 1) * np, np * 3 * sizeof(float)), "wrk_memcpy_dtoh");
             if (g != 1.0f)
-                for (size_t i = 0; i < np; ++i) guides[k][i] = guides[k][i] * g;
+                for (size_t i = 0; i < 3 * np; ++i) guides[k][i] = guides[k][i] * g;
         }
     }
     m_impl->stats.paths = st.paths;
     m_impl->stats.extensionRays = st.extensionRays;
     m_impl->stats.shadowRays = st.shadowRays;
+    m_impl->stats.shadowTraced = st.shadowTraced;
     m_impl->stats.iterations = st.iterations;
     m_impl->stats.gpuMs = st.gpuMs;
     m_impl->stats.totalMs = st.totalMs;
-}
-
-// renderer.cpp:318-335
-void Renderer::render(Scene* scene, const Camera& camera, Vec3* out, uint32_t width, uint32_t height, uint32_t spp,
-                      bool denoiser) {
-    RenderParams p;
-    p.width = width;
-    p.height = height;
-    p.spp = spp;
-    p.denoiser.enabled = denoiser;
-    p.denoiser.useAlbedo = true;
-    p.denoiser.useNormal = true;
-    render(scene, camera, out, p);
 }
 
 }  // namespace wr
@@ -687,17 +633,4 @@ extern "C" int wrk_hdr_write(const char* path, const float* rgb, uint32_t width,
     return write_file(path, o, "hdr");
 }
 
-namespace test_helpers {
-void savePNG(const char* filename, const wr::Vec3* image, uint32_t width, uint32_t height) {
-    int rc = wrk_image_save_png(filename, reinterpret_cast<const float*>(image), width, height);
-    if (rc) throw std::runtime_error(std::string("savePNG(") + (filename ? filename : "") + "): " + wrk_last_error());
-}
-void saveEXR(const char* filename, const wr::Vec3* image, uint32_t width, uint32_t height) {
-    int rc = wrk_exr_write(filename, reinterpret_cast<const float*>(image), width, height);
-    if (rc) throw std::runtime_error(std::string("saveEXR(") + (filename ? filename : "") + "): " + wrk_last_error());
-}
-void saveHDR(const char* filename, const wr::Vec3* image, uint32_t width, uint32_t height) {
-    int rc = wrk_hdr_write(filename, reinterpret_cast<const float*>(image), width, height);
-    if (rc) throw std::runtime_error(std::string("saveHDR(") + (filename ? filename : "") + "): " + wrk_last_error());
-}
-}  // namespace test_helpers
+

@@ -140,7 +140,8 @@ struct Counters {
     uint32_t activeSlots;  // slots still active after this iteration's completion check
     uint32_t iterLimit;    // the device-driven loop stops after this many iterations
     unsigned long long extRays;
-    unsigned long long shdRays;
+    unsigned long long shdRays;    // shadow queries: traced + answered in the Lambert shade
+    unsigned long long shdTraced;  // shadow queries traced by the any-hit kernel
     unsigned long long paths;
     unsigned long long bucketTotal[kNumBuckets];
 };

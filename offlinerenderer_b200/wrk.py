@@ -56,7 +56,7 @@ class RenderStatsC(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("extensionRays", C.c_uint64), ("shadowRays", C.c_uint64),
                 ("iterations", C.c_uint32), ("deviceErrors", C.c_uint32), ("gpuMs", C.c_float),
                 ("totalMs", C.c_float), ("stageMs", C.c_float * 9), ("stageLaunches", C.c_uint32 * 9),
-                ("bucketPaths", C.c_uint64 * 5)]
+                ("bucketPaths", C.c_uint64 * 5), ("shadowTraced", C.c_uint64)]
 
 
 class BvhInfoC(C.Structure):

@@ -74,7 +74,9 @@ void orc_render(void* s, const orc_camera* cam, const orc_render_params* p, floa
 
 // Ray queries.  rays: 8 floats each (ox,oy,oz,tmin,dx,dy,dz,tmax).
 // out_t/out_prim: closest hit (prim 0xffffffff on miss).  mode 0 = FP32
-// Moller-Trumbore via the BVH, 1 = FP64 over all triangles (exact reference).
+// Moller-Trumbore via the BVH, 1 = FP64 over all triangles (exact reference),
+// 2 = the same FP64 test on the triangles a BVH walk with conservatively widened
+// FP64 boxes reaches (equal to mode 1, fast enough for millions of triangles).
 void orc_closest(void* s, const float* rays, uint32_t n, int mode, float* out_t, uint32_t* out_prim,
                  int threads);
 void orc_occluded(void* s, const float* rays, uint32_t n, uint32_t* out, int threads);

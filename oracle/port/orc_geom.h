@@ -317,6 +317,61 @@ __attribute__((target_clones("fma", "default"))) static bool closest32(const Sce
     return pb != 0xffffffffu;
 }
 
+// FP64 slab test against the FP32 box (which bounds the FP32 vertices exactly),
+// widened by a relative 1e-9 plus an absolute 1e-12 on both ends: far more than the
+// ~1e-16 relative rounding of the double arithmetic, so no box whose triangles the
+// exact test hits is ever culled.
+inline bool box_hit64(const BNode& b, const double o[3], const double inv[3], double tmin, double tmax) {
+    double t0 = tmin, t1 = tmax;
+    for (int k = 0; k < 3; ++k) {
+        double a = ((double)b.lo[k] - o[k]) * inv[k], c = ((double)b.hi[k] - o[k]) * inv[k];
+        double n = std::min(a, c), f = std::max(a, c);
+        if (n != n) n = -INFINITY;  // 0*inf
+        if (f != f) f = INFINITY;
+        t0 = std::max(t0, n);
+        t1 = std::min(t1, f);
+    }
+    return t0 - (std::fabs(t0) * 1e-9 + 1e-12) <= t1 + (std::fabs(t1) * 1e-9 + 1e-12);
+}
+
+// Exact-reference closest hit: the FP64 Moller-Trumbore of every triangle a ray can
+// reach, found by walking the CPU BVH with the widened FP64 slab test above (the
+// result equals testing all triangles, without the O(triangles) cost per ray).
+// Ties in t go to the lower triangle index.
+static bool closest64(const Scene& s, const double o[3], const double d[3], double tmin, double tmax, double& tb,
+                      uint32_t& pb) {
+    double inv[3] = {1.0 / d[0], 1.0 / d[1], 1.0 / d[2]};
+    tb = tmax;
+    pb = 0xffffffffu;
+    uint32_t st[128];
+    int sp = 0;
+    st[sp++] = 0;
+    while (sp) {
+        const BNode& nd = s.nodes[st[--sp]];
+        if (!box_hit64(nd, o, inv, tmin, tb)) continue;
+        if (nd.count) {
+            for (uint32_t i = 0; i < nd.count; ++i) {
+                uint32_t p = s.primOrder[nd.left + i];
+                // edges recomputed in double from the vertices (the FP32 edge arrays are rounded)
+                V3f va = s.vert(s.idx[3 * (size_t)p]), vb = s.vert(s.idx[3 * (size_t)p + 1]),
+                    vc = s.vert(s.idx[3 * (size_t)p + 2]);
+                double v0[3] = {va.x, va.y, va.z};
+                double e1[3] = {(double)vb.x - va.x, (double)vb.y - va.y, (double)vb.z - va.z};
+                double e2[3] = {(double)vc.x - va.x, (double)vc.y - va.y, (double)vc.z - va.z};
+                double t;
+                if (mt64(o, d, v0, e1, e2, t) && t >= tmin && t <= tmax && (t < tb || (t == tb && p < pb))) {
+                    tb = t;
+                    pb = p;
+                }
+            }
+        } else {
+            st[sp++] = nd.left;
+            st[sp++] = nd.left + 1;
+        }
+    }
+    return pb != 0xffffffffu;
+}
+
 __attribute__((target_clones("fma", "default"))) static bool occluded32(const Scene& s, const float o[3],
                                                                        const float d[3], float tmin, float tmax) {
     float inv[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};

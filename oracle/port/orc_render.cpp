@@ -12,7 +12,9 @@
 //   * the host wavefront loop (per-path view)          libWR/src/internal/renderer.cpp:190-313
 // OptiX traversal is replaced by a CPU binned-SAH BVH with a Moller-Trumbore test
 // whose FP32 arithmetic is the same formula the CUDA trace kernel evaluates; the
-// FP64 mode of orc_closest tests every triangle in double precision.
+// FP64 modes of orc_closest are the exact reference: mode 1 tests every triangle in
+// double precision, mode 2 walks the BVH with conservatively widened FP64 boxes
+// (the same answer in O(log n) per ray, for multi-million-triangle scenes).
 #include "orc_geom.h"
 
 #include <atomic>
@@ -528,6 +530,13 @@ void orc_closest(void* sp, const float* rays, uint32_t n, int mode, float* out_t
             uint32_t p;
             closest32(*s, o, d, r[3], r[7], t, p);
             out_t[i] = (p == 0xffffffffu) ? INFINITY : t;
+            out_prim[i] = p;
+        } else if (mode == 2) {
+            double od[3] = {o[0], o[1], o[2]}, dd[3] = {d[0], d[1], d[2]};
+            double t;
+            uint32_t p;
+            closest64(*s, od, dd, r[3], r[7], t, p);
+            out_t[i] = (p == 0xffffffffu) ? INFINITY : (float)t;
             out_prim[i] = p;
         } else {
             double od[3] = {o[0], o[1], o[2]}, dd[3] = {d[0], d[1], d[2]};

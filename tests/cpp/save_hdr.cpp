@@ -3,6 +3,7 @@
 #include <cstdio>
 #include <vector>
 
+#include "wr/image.h"
 #include "wr/wr.h"
 
 int main(int argc, char** argv) {

@@ -32,12 +32,44 @@ def test_binding_covers_every_declared_symbol(wrk_lib):
 
 
 def test_cpp_api_symbols_exported(wrk_lib):
+    """The compiled part of the C++ API is exported, and none of it names Vec3,
+    Camera, RenderParams or GLM: the members that take those are inline in
+    include/wr, so one libwrk.so serves callers built with glm::vec3 (libWR's
+    wr::Vec3) and with the GLM-free fallback."""
     out = subprocess.run(["nm", "-DC", "--defined-only", wrk_lib.LIB_PATH], capture_output=True, text=True).stdout
     for sym in ["wr::Scene::addTriangleMesh(std::span<float const", "wr::Scene::finalize(wr::SceneBuildConfig const&)",
-                "wr::Renderer::render(wr::Scene*, wr::Camera const&, wr::Vec3*, wr::RenderParams const&)",
+                "wr::Renderer::renderNative(wr::Scene*, wrk_camera const&, wrk_render_params const&, float*, float*, "
+                "float*, bool, char const*)",
                 "wr::Context::createScene()", "wr::Texture2D::create(wr::Scene*",
-                "wr::Scene::addGGXTransmissionMaterial(wr::Vec3 const&, float, float)"]:
+                "wr::Scene::addMaterialRecord(wrk_material const&)",
+                "wr::Scene::setEnvironmentRadianceRGB(float, float, float)"]:
         assert sym in out, sym
+    wr_syms = [ln for ln in out.splitlines() if " wr::" in ln or " test_helpers::" in ln]
+    assert wr_syms
+    for ln in wr_syms:
+        assert not re.search(r"Vec3|glm|wr::Camera|RenderParams", ln), ln
+
+
+GLM_DIRS = [os.environ.get("WR_GLM_INCLUDE", ""), os.path.join(ROOT, "..", "reference", "libWR", "external")]
+
+
+@pytest.mark.parametrize("glm", [False, True])
+def test_cpp_api_compiles_and_links_with_and_without_glm(wrk_lib, tmp_path, glm):
+    """A libWR-style program (GLM math on wr::Vec3, Camera's GLM helpers when GLM is
+    present) compiles against include/wr and links against libwrk.so both ways."""
+    flags = []
+    if glm:
+        found = [d for d in GLM_DIRS if d and os.path.exists(os.path.join(d, "glm", "glm.hpp"))]
+        if not found:
+            pytest.skip("GLM headers not found (set WR_GLM_INCLUDE)")
+        flags = ["-I", found[0], "-DWR_EXPECT_GLM"]
+    else:
+        flags = ["-DWR_NO_GLM"]
+    lib_dir = os.path.dirname(wrk_lib.LIB_PATH)
+    r = subprocess.run(["g++", "-std=c++20", "-O1", "-I", os.path.join(ROOT, "include")] + flags +
+                       [os.path.join(ROOT, "tests", "cpp", "api_types.cpp"), "-o", str(tmp_path / "api_types"),
+                        "-L", lib_dir, "-lwrk", f"-Wl,-rpath,{lib_dir}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
 
 
 def test_no_device_fails_loudly(wrk_lib):

@@ -43,6 +43,33 @@ def test_cdf_selection_bitexact(gpu, oracle):
         assert np.array_equal(gpu.cdf_sample(cdf, u), oracle.cdf_sample(cdf, u))
 
 
+@pytest.mark.parametrize("name", ["cornell", "showcase", "scale"])
+def test_scene_light_cdf_bitexact(gpu, oracle, name):
+    """The emissive list and power CDF the product builds at finalize (read back
+    from the device through wrk_scene_light_cdf) equal the oracle's restatement of
+    scene.cpp:423-491 bit for bit -- on the Cornell box (2 equal lights), the
+    material showcase, and the full 1920x1080 scale scene (~2.41M triangles, 64
+    lights of unequal power) -- and light selection on that device CDF matches
+    the oracle's for the same uniforms."""
+    make = {"cornell": lambda: scenes.cornell(64, 64, 1, seed=1),
+            "showcase": lambda: scenes.material_showcase(64, 64, 1, seed=1),
+            "scale": lambda: scenes.scale_test(1920, 1080, 1, seed=1)}[name]
+    sd = make()
+    sc = gpu.Scene.from_data(sd)
+    tris, cdf = sc.light_cdf()
+    otris, ocdf = oracle.scene(sd).light_cdf()
+    assert len(tris) == len(otris) > 0
+    assert np.array_equal(tris, otris)
+    assert np.array_equal(cdf.view(np.uint32), ocdf.view(np.uint32))
+    if name == "scale":
+        assert len(tris) == 64
+        power = np.diff(np.concatenate([[0.0], ocdf.astype(np.float64)]))
+        assert power.max() > 2.0 * power.min()  # the lights really differ in power
+    u = np.random.default_rng(9).random(200000).astype(np.float32)
+    u[:len(cdf)] = cdf  # u equal to a CDF value: the lower bound's tie case
+    assert np.array_equal(gpu.cdf_sample(cdf, u), oracle.cdf_sample(ocdf, u))
+
+
 def test_compaction_bitexact(gpu, oracle):
     rng = np.random.default_rng(3)
     for n in (0, 1, 31, 1024, 1025, 100003, 1 << 21):
@@ -54,47 +81,92 @@ def test_compaction_bitexact(gpu, oracle):
     assert len(gpu.compact(stage, np.arange(5000, dtype=np.uint32))) == 0
 
 
+# Level-1 bound (north star): every finite BSDF / sampling / MIS output within 1e-5
+# relative of the FP64 transcription of the reference's formulas.  Records are left
+# out only by a computed condition criterion: where the reference's OWN FP32
+# arithmetic (the oracle's FP32 port, bit-identical to the reference build compiled
+# on the host) already differs from FP64 by more than half the tolerance, the
+# quantity is ill-conditioned in FP32 at that input -- e.g. the GGX D term near its
+# peak at low roughness, where 1 - NoH^2 (1 - a^2) cancels and amplifies the
+# rounding of NoH by ~1/a^2 -- and no FP32 evaluation of the same formula can be
+# held to 1e-5 there.  The excluded fraction is capped per column below (measured
+# on these seeded inputs; roughness U(0.05, 1)).
+TOL = 1e-5
+COND = 0.5 * TOL
+BSDF_COLS = [c for c in range(34) if c not in (8, 16)]  # 8, 16: integer outputs
+# per-column cap on the excluded fraction: the VNDF sample pdf (7) is the D term at
+# the sampled half-vector, ill-conditioned for roughness below ~0.3
+EXCLUDE_CAP = {7: 0.30}
+EXCLUDE_CAP_DEFAULT = 0.02
+
+
+def _rel(x, r):
+    with np.errstate(divide="ignore", invalid="ignore"):
+        d = np.abs(x - r) / np.abs(r)
+    d[(r == 0) & (x == 0)] = 0.0
+    d[(r == 0) & (x != 0)] = np.inf
+    return d
+
+
+def _check_against_fp64(g, o32, o64, label):
+    """Max relative error of g vs o64 over the well-conditioned finite records of
+    every column; returns {column: (max error, excluded fraction)}."""
+    report = {}
+    for c in BSDF_COLS:
+        fin = np.isfinite(o64[:, c]) & np.isfinite(o32[:, c])
+        # non-finite where the reference is non-finite (e.g. the 0/0 pdf of A14), nowhere else
+        assert np.array_equal(np.isfinite(g[:, c]), fin), (label, c)
+        cond = fin & (_rel(o32[:, c], o64[:, c]) <= COND)
+        excluded = 1.0 - cond.sum() / max(1, fin.sum())
+        assert excluded <= EXCLUDE_CAP.get(c, EXCLUDE_CAP_DEFAULT), (label, c, excluded)
+        err = float(_rel(g[cond, c], o64[cond, c]).max()) if cond.any() else 0.0
+        report[c] = (err, excluded)
+        assert err < TOL, (label, c, err, excluded)
+    return report
+
+
 def test_bsdf_fp32_vs_oracle(gpu, oracle):
+    """The device's FP32 shading math against the oracle's FP32 restatement (the
+    reference's expression order, correctly rounded operations): integer outputs
+    are identical, nearly every value is bit-identical, and where CUDA's and
+    glibc's sin / cos / pow differ by an ulp the difference stays inside 1e-5 on
+    every well-conditioned record."""
     import pyoracle
 
     inp = pyoracle.random_bsdf_inputs(200000, seed=11)
     g = gpu.bsdf_batch(inp).astype(np.float64)
     o = oracle.bsdf(inp, 0)
+    o64 = oracle.bsdf(inp, 1)
     same = (g == o) | (np.isnan(g) & np.isnan(o))
-    # integer-valued outputs (sample success, RR decision) are exact
     assert same[:, 8].all() and same[:, 16].all()
-    # transcendentals (sin/cos/pow) may round differently by a few ulps
     assert same.mean() > 0.97
-    ok = np.isfinite(g) & np.isfinite(o)
-    rel = np.abs(g[ok] - o[ok]) / np.maximum(np.abs(o[ok]), 1e-30)
-    assert np.quantile(rel, 0.999) < 1e-5
+    for c in BSDF_COLS:
+        fin = np.isfinite(o[:, c]) & np.isfinite(o64[:, c])
+        cond = fin & (_rel(o[:, c], o64[:, c]) <= COND)
+        assert float(_rel(g[cond, c], o[cond, c]).max()) < TOL, c
 
 
 def test_bsdf_vs_fp64_transcription(gpu, oracle):
-    """1e-5 relative to the FP64 transcription.  Records near
-    the GGX peak at low roughness are ill-conditioned in FP32 (the reference's own
-    arithmetic loses digits there), so the bound is checked on the 99th
-    percentile and every output is checked against the FP32 oracle above."""
+    """North-star level 1: the maximum (not a percentile) relative error against
+    the FP64 transcription over every well-conditioned finite record is below
+    1e-5, for every output column."""
     import pyoracle
 
     inp = pyoracle.random_bsdf_inputs(100000, seed=12)
     g = gpu.bsdf_batch(inp).astype(np.float64)
-    o = oracle.bsdf(inp, 1)
-    cols = [0, 1, 2, 3, 9, 10, 11, 12, 13, 14, 15, 17, 18, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32, 33]
-    for c in cols:
-        ok = np.isfinite(g[:, c]) & np.isfinite(o[:, c]) & (np.abs(o[:, c]) > 1e-6)
-        rel = np.abs(g[ok, c] - o[ok, c]) / np.abs(o[ok, c])
-        assert np.quantile(rel, 0.99) < 1e-5, (c, np.quantile(rel, 0.99))
+    report = _check_against_fp64(g, oracle.bsdf(inp, 0), oracle.bsdf(inp, 1), "random")
+    worst = max(report.values())
+    print("level-1 max rel error vs FP64 over well-conditioned records:", worst)
 
 
-def test_golden_bsdf_fixture(gpu):
+def test_golden_bsdf_fixture(gpu, oracle):
+    """The golden records the reference build produced (tests/golden/bsdf_ref.npz):
+    integer outputs identical, every well-conditioned output within 1e-5 of FP64."""
     d = np.load(os.path.join(GOLDEN, "bsdf_ref.npz"))
     g = gpu.bsdf_batch(d["inputs"]).astype(np.float64)
     o = d["outputs"]
     assert np.array_equal(g[:, 8], o[:, 8]) and np.array_equal(g[:, 16], o[:, 16])
-    ok = np.isfinite(g) & np.isfinite(o)
-    rel = np.abs(g[ok] - o[ok]) / np.maximum(np.abs(o[ok]), 1e-30)
-    assert np.quantile(rel, 0.999) < 1e-5
+    _check_against_fp64(g, o, oracle.bsdf(d["inputs"], 1), "golden")
 
 
 def test_camera_rays_bitexact(gpu, oracle):

@@ -1,0 +1,190 @@
+"""Drop-in proof: libWR's own test programs run unmodified on this library.
+
+oracle/Makefile compiles libWR's three test mains (trianglestrip/OfflineRenderer
+libWR/test/cornell_box_var_test.cpp, material_showcase_test.cpp,
+rough_glass_test.cpp) and their helpers (geometry / file / image .cpp) straight
+from the reference checkout, against this repository's include/wr headers with
+the reference's vendored GLM on the include path -- so wr::Vec3 is glm::vec3 and
+the programs' glm::radians / GLM arithmetic compile as they do against libWR --
+and links them with libwrk.so.  The only addition is oracle/ref_main_shim.cpp,
+which records the float image each program passes to savePNG and the scene,
+camera and parameters it hands the renderer (see its header).
+
+Each program runs in a temporary directory with a render_config.ini of its own
+section (small size, denoiser off), exactly as the reference reads it
+(libWR/test/helpers/config.h).  Checks:
+  * the program exits 0 and writes its PNG through libWR's own savePNG;
+  * the recorded scene carries the materials and camera the program's source sets;
+  * the float image matches the oracle's render of the recorded scene at the same
+    seed and spp within 1% of the seed-to-seed noise (the level-3 bound of
+    tests/test_gpu_render.py);
+  * the PNG's bytes are the ACES tone map of that float image.
+
+The programs are built only where the reference checkout exists; elsewhere this
+module is skipped.
+"""
+import os
+import struct
+import subprocess
+import zlib
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from offlinerenderer_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref")
+# program -> (render_config.ini section, gallery file it writes)
+MAINS = {
+    "cornell_box_var_test": ("cornell_box_var", "wr_cornell.png"),
+    "material_showcase_test": ("material_showcase", "wr_material_showcase.png"),
+    "rough_glass_test": ("rough_glass", "wr_rough_glass.png"),
+}
+
+
+def relmse(x, r):
+    x = x.astype(np.float64)
+    r = r.astype(np.float64)
+    return float(np.mean((x - r) ** 2 / (r * r + 1e-2)))
+
+
+def _decode_png(path):
+    """8-bit RGB / RGBA PNG (any of the five scanline filters) -> (H, W, C) uint8."""
+    d = open(path, "rb").read()
+    assert d[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, idat, w = 8, b"", 0
+    while pos < len(d):
+        n, typ = struct.unpack(">I4s", d[pos:pos + 8])
+        body = d[pos + 8:pos + 8 + n]
+        if typ == b"IHDR":
+            w, h, depth, ctype = struct.unpack(">IIBB", body[:10])
+            assert depth == 8 and ctype in (2, 6)
+            ch = 3 if ctype == 2 else 4
+        elif typ == b"IDAT":
+            idat += body
+        pos += 12 + n
+    raw = np.frombuffer(zlib.decompress(idat), np.uint8).reshape(h, 1 + w * ch)
+    out = np.zeros((h, w * ch), np.int32)
+    prev = np.zeros(w * ch, np.int32)
+    for y in range(h):
+        f, line = raw[y, 0], raw[y, 1:].astype(np.int32)
+        cur = np.zeros(w * ch, np.int32)
+        for x in range(w * ch):
+            a = cur[x - ch] if x >= ch else 0
+            b = prev[x]
+            c = prev[x - ch] if x >= ch else 0
+            if f == 0:
+                p = 0
+            elif f == 1:
+                p = a
+            elif f == 2:
+                p = b
+            elif f == 3:
+                p = (a + b) >> 1
+            else:
+                pa, pb, pc = abs(b - c), abs(a - c), abs(a + b - 2 * c)
+                p = a if (pa <= pb and pa <= pc) else (b if pb <= pc else c)
+            cur[x] = (line[x] + p) & 255
+        out[y] = cur
+        prev = cur
+    return out.astype(np.uint8).reshape(h, w, ch)
+
+
+def _read_capture(path):
+    d = open(path, "rb").read()
+    assert d[:8] == b"WRCAPT01"
+    pos = 8
+    cam = struct.unpack("<13f", d[pos:pos + 52])
+    pos += 52
+    rp = struct.unpack("<5I2f4I", d[pos:pos + 44])
+    pos += 44
+    denoise, = struct.unpack("<I", d[pos:pos + 4])
+    pos += 4
+    env = struct.unpack("<3f", d[pos:pos + 12])
+    pos += 12
+    arrays = []
+    for dtype in ("<f4", "<f4", "<f4", "<u4", "<u4", scenes.MATERIAL_DTYPE):
+        n, = struct.unpack("<Q", d[pos:pos + 8])
+        pos += 8
+        nbytes = n * np.dtype(dtype).itemsize
+        arrays.append(np.frombuffer(d[pos:pos + nbytes], dtype).copy())
+        pos += nbytes
+    assert pos == len(d)
+    vtx, nrm, uvs, idx, tri_mat, mats = arrays
+    camera = scenes.Camera(position=cam[0:3], target=cam[3:6], up=cam[6:9], fovY=cam[9], aspect=cam[10],
+                           focalDistance=cam[11], lensRadius=cam[12])
+    width, height, spp, use_nee, max_bounces, rr, clamp, seed, max_iter, flags, offset = rp
+    settings = scenes.RenderSettings(width, height, spp, maxBounces=max_bounces, russianRouletteDepth=rr,
+                                     useNEE=bool(use_nee), fireflyClamp=clamp, seed=seed)
+    sd = scenes.SceneData(vertices=vtx.reshape(-1, 3), indices=idx.reshape(-1, 3), tri_material=tri_mat,
+                          materials=mats, normals=nrm.reshape(-1, 3) if len(nrm) else None,
+                          uvs=uvs.reshape(-1, 2) if len(uvs) else None, env=env, camera=camera, settings=settings)
+    return sd, {"maxIterations": max_iter, "flags": flags, "sampleOffset": offset, "denoise": denoise}
+
+
+def _run_main(prog, section, tmp_path, width, height, spp):
+    exe = os.path.join(REF_BIN, prog)
+    (tmp_path / "render_config.ini").write_text(
+        f"[{section}]\nwidth = {width}\nheight = {height}\nspp = {spp}\ndenoiser = 0\n")
+    (tmp_path / "gallery").mkdir()
+    r = subprocess.run([exe], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return r.stdout
+
+
+@pytest.fixture(scope="module")
+def programs():
+    missing = [p for p in MAINS if not os.path.exists(os.path.join(REF_BIN, p))]
+    if missing:
+        pytest.skip(f"libWR test programs not built (needs the reference checkout): {missing}")
+    return REF_BIN
+
+
+@pytest.mark.parametrize("prog", list(MAINS))
+def test_reference_main_matches_oracle(gpu, oracle, programs, prog, tmp_path):
+    section, png_name = MAINS[prog]
+    width, height, spp = 64, 48, 8
+    _run_main(prog, section, tmp_path, width, height, spp)
+    sd, extra = _read_capture(tmp_path / "wr_capture.bin")
+    png = tmp_path / "gallery" / png_name
+    raw = np.fromfile(str(png) + ".f32", np.uint8)
+    w, h = struct.unpack("<2I", raw[:8].tobytes())
+    img = raw[8:].view(np.float32).reshape(h, w, 3)
+
+    # what the program's source sets (libWR/test/*_test.cpp main and scene builder)
+    st, cam = sd.settings, sd.camera
+    assert (st.width, st.height, st.spp) == (width, height, spp) == (w, h, spp)
+    assert st.maxBounces == 12 and st.russianRouletteDepth == 5.0 and st.useNEE and st.seed == 0
+    assert extra == {"maxIterations": 8, "flags": 0, "sampleOffset": 0, "denoise": 0}
+    assert np.float32(cam.aspect) == np.float32(width) / np.float32(height)
+    fov = {"cornell_box_var": 45.0, "material_showcase": 50.0, "rough_glass": 45.0}[section]
+    assert np.float32(cam.fovY) == scenes._radians(fov)
+    m = sd.materials
+    emissive = m[m["type"] == scenes.EMISSIVE]
+    assert len(emissive) == 1
+    light = {"cornell_box_var": 15.0, "material_showcase": 20.0, "rough_glass": 15.0}[section]
+    assert np.all(emissive["emission"][0][:3] == np.float32(light))
+    if section == "cornell_box_var":
+        assert len(m) == 7 and m["albedoTextureId"][0] == 1
+        gold = m[m["type"] == scenes.GGX_REFLECTION][0]
+        assert gold["roughness"] == np.float32(0.2) and gold["metallic"] == 1.0
+        assert tuple(cam.position) == (0.0, 1.5, 4.5)
+        # the floor's checker texture, as Texture2D::create loaded it from the PNG
+        sd.textures = [np.ascontiguousarray(_decode_png(os.path.join(REF_BIN, "res", "checkerboard_line.png")))]
+        assert sd.textures[0].shape == (64, 64, 4)
+    assert sd.num_triangles > 100
+
+    # the image: the oracle's render of the same scene, same seed and spp
+    osc = oracle.scene(sd)
+    o_rgb, _, _, _ = osc.render()
+    st2 = scenes.RenderSettings(**{**st.__dict__, "seed": 101})
+    noise = relmse(osc.render(settings=st2)[0], o_rgb)
+    assert np.isfinite(img).all() and img.mean() > 1e-3
+    err = relmse(img, o_rgb)
+    assert err < 0.01 * noise, (prog, err, noise)
+
+    # the PNG: libWR's own writer applied to that float image
+    assert np.array_equal(_decode_png(png), oracle.tonemap(img.reshape(-1, 3)).reshape(h, w, 3))

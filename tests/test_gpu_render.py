@@ -24,6 +24,9 @@ CASES = {
     "cornell": lambda: scenes.cornell(64, 64, 16, seed=1),
     "showcase": lambda: scenes.material_showcase(64, 64, 8, seed=1, tex_size=256),
     "scale_small": lambda: scenes.scale_test(48, 32, 4, grid=96, spheres=30, lights=16, seed=2),
+    # the full scale scene (1024^2 fBm heightfield + 250 icospheres, ~2.41M triangles,
+    # 64 lights of unequal power) at a small image size
+    "scale_full": lambda: scenes.scale_test(64, 36, 4, seed=1),
 }
 
 

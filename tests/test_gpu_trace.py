@@ -1,8 +1,11 @@
 """Closest-hit and visibility parity of the GPU BVH traversal.
 
 Against the oracle's FP32 Moller-Trumbore (same arithmetic): primitive ids and t
-agree exactly.  Against the FP64 exact intersector over all triangles: primitive
-ids agree on >= 99.99% of rays and t within 1e-5 relative (north-star level 2).
+agree exactly.  Against the FP64 exact intersector: primitive ids agree on
+>= 99.99% of rays and t within 1e-5 relative wherever both hit (north-star level
+2).  The exact intersector tests every triangle in FP64 (oracle mode 1); on the
+2.41M-triangle scale scene it reaches the triangles by walking the oracle's CPU
+BVH with conservatively widened FP64 boxes (mode 2, checked equal to mode 1).
 """
 import numpy as np
 import pytest
@@ -52,12 +55,22 @@ def test_closest_hit_vs_fp64_exact(gpu, oracle):
     s = gpu.Scene.from_data(sd)
     rays = np.concatenate([random_rays(sd, 40000, 3), camera_like_rays(oracle, sd, 20000, 4)])
     t, p = s.trace_closest(rays)
-    t64, p64 = oracle.scene(sd).closest(rays, mode=1)
+    osc = oracle.scene(sd)
+    t64, p64 = osc.closest(rays, mode=1)
+    _check_level2(t, p, t64, p64)
+    t2, p2 = osc.closest(rays, mode=2)
+    assert np.array_equal(p2, p64) and np.array_equal(t2, t64)
+
+
+def _check_level2(t, p, t64, p64):
+    miss = np.uint32(0xFFFFFFFF)
     agree = (p == p64).mean()
     assert agree >= 0.9999, agree
-    hit = (p == p64) & (p != 0xFFFFFFFF)
-    rel = np.abs(t[hit].astype(np.float64) - t64[hit]) / np.abs(t64[hit])
-    assert rel.max() < 1e-5
+    both = (p != miss) & (p64 != miss)
+    assert ((p != miss) == (p64 != miss)).mean() >= 0.9999
+    rel = np.abs(t[both].astype(np.float64) - t64[both]) / np.abs(t64[both])
+    assert rel.max() < 1e-5, rel.max()
+    return agree
 
 
 def test_occlusion_matches_oracle(gpu, oracle):
@@ -114,17 +127,25 @@ def test_many_identical_triangles(gpu, oracle):
     assert np.array_equal(p, po) and np.array_equal(t, to)
 
 
-def test_large_scene_against_fp64_sample(gpu, oracle):
-    """About 2.4M triangles (the scale-test scene): the BVH builds and a sample of
-    rays agrees with the exact FP64 intersector."""
-    sd = scenes.scale_test(64, 36, 1)
+def test_large_scene_against_fp64(gpu, oracle):
+    """The full scale-test scene (1920x1080 camera, 1024^2 fBm heightfield + 250
+    icospheres, ~2.41M triangles): 100k camera rays of the benchmark camera and
+    100k random rays.  Bit-exact against the FP32 oracle; against the FP64 exact
+    intersector (BVH walk, mode 2) >= 99.99% primitive-id agreement and t within
+    1e-5 relative; mode 2 equals the all-triangle FP64 test on a sample."""
+    sd = scenes.scale_test(1920, 1080, 1, seed=1)
     s = gpu.Scene.from_data(sd)
     info = s.bvh_info()
     assert info["numTriangles"] == sd.num_triangles > 2_000_000
-    rays = camera_like_rays(oracle, sd, 2000, 9)
+    rays = np.concatenate([camera_like_rays(oracle, sd, 100000, 9), random_rays(sd, 100000, 10)])
     t, p = s.trace_closest(rays)
     osc = oracle.scene(sd)
     to, po = osc.closest(rays, mode=0)
     assert np.array_equal(p, po) and np.array_equal(t, to)
-    t64, p64 = osc.closest(rays[:300], mode=1)
-    assert (p[:300] == p64).mean() >= 0.99
+    t64, p64 = osc.closest(rays, mode=2)
+    agree = _check_level2(t, p, t64, p64)
+    assert (p[:100000] != 0xFFFFFFFF).mean() > 0.3  # the terrain fills ~44% of the benchmark view
+    sample = np.r_[0:32, 100000:100032]
+    t1, p1 = osc.closest(rays[sample], mode=1)
+    assert np.array_equal(p1, p64[sample]) and np.array_equal(t1, t64[sample])
+    print(f"level 2 on the scale scene: {agree:.6f} primitive-id agreement over {len(rays)} rays")

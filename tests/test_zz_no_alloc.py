@@ -45,6 +45,21 @@ def test_noalloc_compaction_matches_allocating_entry_point(gpu):
         assert np.array_equal(got, idx[stage[idx] != 3])
 
 
+def test_noalloc_compaction_at_tile_boundaries(gpu):
+    """Exact multiples of the 1024-entry tile: one tile, 1024 tiles (the scan's
+    first carry into a second chunk of tile counts) and 65,536 tiles, the largest
+    input the fixed scratch accepts (256 MiB per index buffer)."""
+    L = gpu.lib()
+    rng = np.random.default_rng(7)
+    for n in (1024, 1024 * 1024, 1024 * 1024 + 1, 65536 * 1024):
+        stage = rng.integers(0, 4, n, dtype=np.uint32)
+        idx = rng.permutation(n).astype(np.uint32)
+        got = _compact_via("wrk_compact_noalloc", L, stage, idx)
+        assert np.array_equal(got, idx[stage[idx] != 3]), n
+        want = _compact_via("wrk_compact", L, stage, idx)
+        assert np.array_equal(got, want), n
+
+
 def test_noalloc_compaction_rejects_sizes_beyond_its_scratch(gpu):
     L = gpu.lib()
     wrk = gpu
@@ -53,6 +68,10 @@ def test_noalloc_compaction_rejects_sizes_beyond_its_scratch(gpu):
     too_many = 65536 * 1024 + 1  # rejected before any buffer is touched
     rc = L.wrk_compact_noalloc(small.ptr, small.ptr, too_many, small.ptr, count.ptr)
     assert rc == 1  # WRK_ERR_INVALID
+    assert b"scratch limit" in L.wrk_last_error()
+    # the largest 32-bit size: its tile count must not wrap to zero and pass
+    rc = L.wrk_compact_noalloc(small.ptr, small.ptr, 0xFFFFFFFF, small.ptr, count.ptr)
+    assert rc == 1
     assert b"scratch limit" in L.wrk_last_error()
     # the empty input is fine and reports zero survivors
     assert L.wrk_compact_noalloc(small.ptr, small.ptr, 0, small.ptr, count.ptr) == 0
