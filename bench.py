@@ -198,11 +198,12 @@ def served_legs(args, rend, local):
     ttr["workload"] = "scale_test 1920x1080 maxDepth8 (~2.41M tris), camera of the benchmark scene, seed 1"
     ttr["reference"] = f"{args.ref_spp} spp, f32 sums per 256-spp chunk accumulated in f64"
     out["time_to_relmse"] = ttr
-    # serving: Poisson arrivals, random orbit cameras, mixed sizes and spp, denoised
+    # serving: Poisson arrivals, orbit cameras from a fixed pose set, mixed sizes and
+    # spp, denoised; every served image scored against an FP64 reference afterwards
     srv = wrk.Server(device=local)
     srv.set_denoiser(dn)
     out["serving"] = serve_bench.run(srv, scene, n_requests=args.serve_requests, rate=50.0, device=local,
-                                     audit_renderer=rend)
+                                     quality_renderer=rend, ref_spp=args.serve_ref_spp)
     out["serving"]["scene"] = "scale_test (~2.41M tris), resident"
     del srv
     return out
@@ -342,7 +343,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=0, help="override the config's spp (smaller profiling cases)")
     ap.add_argument("--no-served", action="store_true", help="skip the denoiser / time-to-relMSE / serving legs")
-    ap.add_argument("--serve-requests", type=int, default=400)
+    ap.add_argument("--serve-requests", type=int, default=1000)
+    ap.add_argument("--serve-ref-spp", type=int, default=1024,
+                    help="spp of the FP64 references the served images are scored against")
     ap.add_argument("--ref-spp", type=int, default=4096)
     args = ap.parse_args()
     cfg = CONFIGS[args.config]

@@ -125,7 +125,7 @@ struct wrk_scene {
     uint32_t envW = 0, envH = 0;
     bool finalized = false;
     DevBuf dEnvMap;
-    DevBuf dVtx, dNrm, dUv, dIdx, dTriMat, dMats, dTexels, dTexInfo, dEmissive, dCdf, dErr;
+    DevBuf dVtx, dNrm, dUv, dIdx, dTriMat, dMats, dTexels, dTexInfo, dEmissive, dCdf, dLights, dErr;
     uint4* nodes = nullptr;
     float4* tris = nullptr;
     std::vector<uint32_t> emissive;
@@ -537,6 +537,23 @@ int wrk_scene_finalize(wrk_scene* s) {
     if (rc) return rc;
     uint32_t nt = (uint32_t)s->triMat.size();
     build_light_cdf(s);
+    // the light records NEE reads after choosing an entry of the CDF: the emissive
+    // triangle's three vertices and its material's emission, in one 64-byte record
+    std::vector<float4> lights;
+    for (uint32_t t : s->emissive) {
+        const float* a = &s->vtx[3 * (size_t)s->idx[3 * (size_t)t]];
+        const float* b = &s->vtx[3 * (size_t)s->idx[3 * (size_t)t + 1]];
+        const float* c = &s->vtx[3 * (size_t)s->idx[3 * (size_t)t + 2]];
+        const wrk_material& m = s->mats[s->triMat[t]];
+        uint32_t tb = t;
+        float tf;
+        std::memcpy(&tf, &tb, sizeof(tf));
+        lights.push_back(make_float4(a[0], a[1], a[2], tf));
+        lights.push_back(make_float4(b[0], b[1], b[2], 0.0f));
+        lights.push_back(make_float4(c[0], c[1], c[2], 0.0f));
+        lights.push_back(make_float4(m.emission[0], m.emission[1], m.emission[2], 0.0f));
+    }
+    if ((rc = upload(s->dLights, lights))) return rc;
     if ((rc = upload(s->dVtx, s->vtx)) || (rc = upload(s->dNrm, s->nrm)) || (rc = upload(s->dUv, s->uv)) ||
         (rc = upload(s->dIdx, s->idx)) || (rc = upload(s->dTriMat, s->triMat)) || (rc = upload(s->dMats, s->mats)) ||
         (rc = upload(s->dEmissive, s->emissive)) || (rc = upload(s->dCdf, s->cdf)))
@@ -583,6 +600,7 @@ int wrk_scene_finalize(wrk_scene* s) {
     v.numTex = (uint32_t)s->tex.size();
     v.emissive = s->dEmissive.as<uint32_t>();
     v.cdf = s->dCdf.as<float>();
+    v.lights = s->dLights.as<float4>();
     v.numEmissive = (uint32_t)s->emissive.size();
     v.numTris = nt;
     for (int k = 0; k < 3; ++k) v.env[k] = s->env[k];

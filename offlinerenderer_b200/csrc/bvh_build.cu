@@ -35,6 +35,9 @@ namespace {
 constexpr int kBins = 16;
 constexpr uint32_t kSmallTask = 16;
 constexpr uint32_t kMaxLeaf = 3;
+// BVH levels (and collapse depths) enqueued between two host reads of the counts.
+constexpr int kLevelsPerSync = 4;
+constexpr uint32_t kMaxLevels = 256;
 
 __host__ __device__ __forceinline__ uint32_t f2o(float f) {
 #ifdef __CUDA_ARCH__
@@ -76,11 +79,13 @@ struct Split {
 struct SmallTask {
     uint32_t node, begin, end, pad;
 };
+// cur: open tasks of the level being built (set on the device from nextTasks at the
+// start of each level, so the host need not read it back between levels).
 struct BuildCtr {
-    uint32_t nodes, nextTasks, small, pad;
+    uint32_t nodes, nextTasks, small, cur;
 };
 struct CollapseCtr {
-    uint32_t nodes, tris, next, maxDepth;
+    uint32_t nodes, tris, next, maxDepth, cur;
 };
 
 __device__ __forceinline__ void obox_empty(OBox& b) {
@@ -127,9 +132,16 @@ __global__ void k_prim_bounds(const float* __restrict__ vtx, const uint32_t* __r
     }
 }
 
-__global__ void k_init_bins(Bin* bins, uint32_t nb) {
+// One thread, at the start of a level: the tasks the last level opened become this
+// level's (the device keeps the count; the host reads it only every few levels).
+__global__ void k_level_begin(BuildCtr* ctr) {
+    ctr->cur = ctr->nextTasks;
+    ctr->nextTasks = 0;
+}
+
+__global__ void k_init_bins(Bin* bins, const BuildCtr* __restrict__ ctr) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nb) return;
+    if (i >= ctr->cur * 3u * kBins) return;
     Bin b;
     b.cnt = 0;
     for (int k = 0; k < 3; ++k) { b.lo[k] = f2o(FLT_MAX); b.hi[k] = f2o(-FLT_MAX); }
@@ -220,11 +232,10 @@ __device__ __forceinline__ float half_area(const float lo[3], const float hi[3])
     return dx * dy + dy * dz + dz * dx;
 }
 
-__global__ void k_split(uint32_t numTasks, const Task* __restrict__ tasks, const Bin* __restrict__ bins,
-                        Split* splits, Task* nextTasks, OBox* nextCen, SmallTask* small, BNode* nodes, OBox* nbox,
-                        BuildCtr* ctr) {
+__global__ void k_split(const Task* __restrict__ tasks, const Bin* __restrict__ bins, Split* splits, Task* nextTasks,
+                        OBox* nextCen, SmallTask* small, BNode* nodes, OBox* nbox, BuildCtr* ctr) {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= numTasks) return;
+    if (t >= ctr->cur) return;
     Task tk = tasks[t];
     uint32_t cnt = tk.end - tk.begin;
     float bestCost = FLT_MAX;
@@ -508,10 +519,10 @@ __global__ void k_fix_boxes(uint32_t numNodes, BNode* nodes, const OBox* __restr
     }
 }
 
-__global__ void k_mark_level_nodes(uint32_t numTasks, const Task* __restrict__ tasks, const Split* __restrict__ splits,
-                                   uint8_t* fromLevels) {
+__global__ void k_mark_level_nodes(const BuildCtr* __restrict__ ctr, const Task* __restrict__ tasks,
+                                   const Split* __restrict__ splits, uint8_t* fromLevels) {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= numTasks) return;
+    if (t >= ctr->cur) return;
     fromLevels[tasks[t].node] = 1;
     fromLevels[splits[t].leftNode] = 1;
     fromLevels[splits[t].leftNode + 1] = 1;
@@ -528,12 +539,18 @@ __device__ __forceinline__ float node_area(const BNode& b) {
     return dx * dy + dy * dz + dz * dx;
 }
 
-__global__ void k_collapse(uint32_t count, const CItem* __restrict__ items, const BNode* __restrict__ bn,
+// One thread, before each collapse depth: last depth's new nodes become this one's items.
+__global__ void k_collapse_begin(CollapseCtr* ctr) {
+    ctr->cur = ctr->next;
+    ctr->next = 0;
+}
+
+__global__ void k_collapse(const CItem* __restrict__ items, const BNode* __restrict__ bn,
                            const uint32_t* __restrict__ ref, const float* __restrict__ vtx,
                            const uint32_t* __restrict__ idx, const uint32_t* __restrict__ triMat, uint4* onodes,
                            float4* otris, CItem* next, CollapseCtr* ctr, uint32_t depth) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
+    if (i >= ctr->cur) return;
     CItem it = items[i];
     uint32_t kids[8];
     int n = 0;
@@ -777,7 +794,7 @@ int build_bvh8(const float* d_vtx, const uint32_t* d_idx, const uint32_t* d_triM
         WRK_BCHECK(cudaMemcpyAsync(tcen, &e, sizeof(OBox), cudaMemcpyHostToDevice, st));
         Task root{0, 0, n, 0};
         WRK_BCHECK(cudaMemcpyAsync(tasks, &root, sizeof(Task), cudaMemcpyHostToDevice, st));
-        BuildCtr c0{1, 0, 0, 0};
+        BuildCtr c0{1, 1, 0, 0};  // the root task is the first level's one task
         WRK_BCHECK(cudaMemcpyAsync(ctr, &c0, sizeof(BuildCtr), cudaMemcpyHostToDevice, st));
     }
     k_prim_bounds<<<grid_for(n, 256), 256, 0, st>>>(d_vtx, d_idx, n, blo, bhi, nbox, tcen);
@@ -791,28 +808,35 @@ int build_bvh8(const float* d_vtx, const uint32_t* d_idx, const uint32_t* d_triM
         WRK_BCHECK(cudaMemcpyAsync(fromLevels, &one, 1, cudaMemcpyHostToDevice, st));
         numTasks = 0;
     }
-    while (numTasks > 0) {
-        uint32_t nb = numTasks * 3 * kBins;
-        k_init_bins<<<grid_for(nb, 256), 256, 0, st>>>(bins, nb);
-        k_bin<<<grid_for(n, 256), 256, 0, st>>>(n, ref, taskOf, tcen, blo, bhi, bins);
-        WRK_BCHECK(cudaMemsetAsync(&ctr->nextTasks, 0, sizeof(uint32_t), st));
-        k_split<<<grid_for(numTasks, 128), 128, 0, st>>>(numTasks, tasks, bins, splits, ntasks, ncen, small, nodes,
-                                                          nbox, ctr);
-        k_mark_level_nodes<<<grid_for(numTasks, 128), 128, 0, st>>>(numTasks, tasks, splits, fromLevels);
-        k_flags<<<grid_for(n, 256), 256, 0, st>>>(n, ref, taskOf, tasks, tcen, splits, blo, bhi, flags);
-        WRK_BCHECK(cub::DeviceScan::ExclusiveSum(cubTmp, cubBytes, flags, scan, (int)n, st));
-        k_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, ref, taskOf, tasks, tcen, splits, blo, bhi, flags, scan, ref2,
-                                                     taskOf2, ncen, nbox);
-        WRK_BCHECK(cudaGetLastError());
+    // Levels run kLevelsPerSync at a time without a host round trip: the device keeps
+    // each level's task count (k_level_begin) and the kernels read it there; the host
+    // sizes grids for an upper bound (a task opens at most two child tasks) and reads
+    // the count back only between batches.  A level with no open task passes every
+    // primitive through unchanged, so the batch may overshoot the last level.
+    for (uint32_t bound = numTasks, levels = 0; numTasks > 0;) {
+        for (int k = 0; k < kLevelsPerSync; ++k, ++levels) {
+            k_level_begin<<<1, 1, 0, st>>>(ctr);
+            k_init_bins<<<grid_for(bound * 3 * kBins, 256), 256, 0, st>>>(bins, ctr);
+            k_bin<<<grid_for(n, 256), 256, 0, st>>>(n, ref, taskOf, tcen, blo, bhi, bins);
+            k_split<<<grid_for(bound, 128), 128, 0, st>>>(tasks, bins, splits, ntasks, ncen, small, nodes, nbox, ctr);
+            k_mark_level_nodes<<<grid_for(bound, 128), 128, 0, st>>>(ctr, tasks, splits, fromLevels);
+            k_flags<<<grid_for(n, 256), 256, 0, st>>>(n, ref, taskOf, tasks, tcen, splits, blo, bhi, flags);
+            WRK_BCHECK(cub::DeviceScan::ExclusiveSum(cubTmp, cubBytes, flags, scan, (int)n, st));
+            k_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, ref, taskOf, tasks, tcen, splits, blo, bhi, flags, scan,
+                                                         ref2, taskOf2, ncen, nbox);
+            WRK_BCHECK(cudaGetLastError());
+            std::swap(ref, ref2);
+            std::swap(taskOf, taskOf2);
+            std::swap(tasks, ntasks);
+            std::swap(tcen, ncen);
+            bound = std::min(maxTasks, 2 * bound);
+        }
         WRK_BCHECK(cudaMemcpyAsync(&hc, ctr, sizeof(BuildCtr), cudaMemcpyDeviceToHost, st));
         WRK_BCHECK(cudaStreamSynchronize(st));
-        std::swap(ref, ref2);
-        std::swap(taskOf, taskOf2);
-        std::swap(tasks, ntasks);
-        std::swap(tcen, ncen);
         numTasks = hc.nextTasks;
-        if (numTasks > maxTasks) {
-            snprintf(err, errlen, "BVH build: task overflow (%u > %u)", numTasks, maxTasks);
+        bound = numTasks;
+        if (numTasks > maxTasks || levels > kMaxLevels) {
+            snprintf(err, errlen, "BVH build: task overflow or level limit (%u tasks, %u levels)", numTasks, levels);
             rc = WRK_ERR_DEVICE;
             goto fail;
         }
@@ -836,22 +860,28 @@ int build_bvh8(const float* d_vtx, const uint32_t* d_idx, const uint32_t* d_triM
     {
         CItem r{0, 0};
         WRK_BCHECK(cudaMemcpyAsync(items, &r, sizeof(CItem), cudaMemcpyHostToDevice, st));
-        CollapseCtr c0{1, 0, 0, 1};
+        CollapseCtr c0{1, 0, 1, 1, 0};  // the root item is the first depth's one item
         WRK_BCHECK(cudaMemcpyAsync(cctr, &c0, sizeof(CollapseCtr), cudaMemcpyHostToDevice, st));
     }
     {
+        // as the binary levels: the item count stays on the device, read back every
+        // kLevelsPerSync depths; an 8-wide node opens at most 8 items
         uint32_t cnt = 1, depth = 1;
         CollapseCtr hcc{};
         while (cnt > 0) {
-            WRK_BCHECK(cudaMemsetAsync(&cctr->next, 0, sizeof(uint32_t), st));
-            k_collapse<<<grid_for(cnt, 64), 64, 0, st>>>(cnt, items, nodes, ref, d_vtx, d_idx, d_triMat, onodes, otris,
-                                                         items2, cctr, depth);
-            WRK_BCHECK(cudaGetLastError());
+            uint32_t bound = cnt;
+            for (int k = 0; k < kLevelsPerSync; ++k) {
+                k_collapse_begin<<<1, 1, 0, st>>>(cctr);
+                k_collapse<<<grid_for(bound, 64), 64, 0, st>>>(items, nodes, ref, d_vtx, d_idx, d_triMat, onodes,
+                                                               otris, items2, cctr, depth);
+                WRK_BCHECK(cudaGetLastError());
+                std::swap(items, items2);
+                ++depth;
+                bound = std::min(numBinary, 8 * bound);
+            }
             WRK_BCHECK(cudaMemcpyAsync(&hcc, cctr, sizeof(CollapseCtr), cudaMemcpyDeviceToHost, st));
             WRK_BCHECK(cudaStreamSynchronize(st));
             cnt = hcc.next;
-            std::swap(items, items2);
-            ++depth;
             if (depth > 256) {
                 snprintf(err, errlen, "BVH collapse: depth limit exceeded");
                 rc = WRK_ERR_DEVICE;

@@ -227,13 +227,25 @@ __device__ __forceinline__ float3 vtx3(const float* v, uint32_t i) {
     return f3(__ldg(v + 3 * i), __ldg(v + 3 * i + 1), __ldg(v + 3 * i + 2));
 }
 
+// The hit triangle's v0, v1 - v0 and v2 - v0 come from its BVH leaf record (at the
+// leaf position the trace kernel stored with the hit: three independent 16-byte
+// loads instead of index -> vertex chains); the builder writes them with correctly
+// rounded subtractions, the same values sub(v1, v0), sub(v2, v0) give.  Indices are
+// loaded only for interpolated normals and uvs.
 __device__ __forceinline__ HitAttr hit_program(const DevScene& s, float3 o, float3 d, float t, uint32_t prim,
-                                               uint32_t mat) {
+                                               uint32_t mat, uint32_t leafPos) {
     HitAttr h;
     float3 hp = f3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
-    uint32_t i0 = __ldg(s.idx + 3 * prim), i1 = __ldg(s.idx + 3 * prim + 1), i2 = __ldg(s.idx + 3 * prim + 2);
-    float3 a = vtx3(s.vtx, i0), b = vtx3(s.vtx, i1), c = vtx3(s.vtx, i2);
-    float3 e1 = sub(b, a), e2 = sub(c, a);
+    const float4* tp = s.tris + 3 * (size_t)leafPos;
+    const float4 ta = __ldg(tp), tb = __ldg(tp + 1), tc = __ldg(tp + 2);
+    uint32_t i0 = 0, i1 = 0, i2 = 0;
+    if (s.nrm || s.uv) {
+        i0 = __ldg(s.idx + 3 * prim);
+        i1 = __ldg(s.idx + 3 * prim + 1);
+        i2 = __ldg(s.idx + 3 * prim + 2);
+    }
+    float3 a = f3(ta.x, ta.y, ta.z);
+    float3 e1 = f3(tb.x, tb.y, tb.z), e2 = f3(tc.x, tc.y, tc.z);
     float3 gn = normalize(cross(e1, e2));
     float3 vp = sub(hp, a);
     float d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(vp, e1), d21 = dot(vp, e2);
@@ -333,14 +345,15 @@ __device__ __forceinline__ bool rr(const Frame& f, PathRegs& r, bool delta) {
 struct LightSample {
     float3 toLight, le;
     float dist, d2, lpdf, cosTheta;
-    uint32_t tri;  // the sampled emissive triangle
+    uint32_t light;  // the sampled entry of the emissive list
 };
+// The light record (emissive list order): v0 | triangle id, v1, v2, emission.
 __device__ __forceinline__ bool sample_light(const DevScene& s, PathRegs& r, const HitAttr& h, LightSample& ls) {
     float lu = rnd_dim(r.seed, r.dim++);
     uint32_t li = cdf_lower_bound(lu, s.cdf, s.numEmissive);
-    uint32_t tri = __ldg(s.emissive + li);
-    uint32_t i0 = __ldg(s.idx + 3 * tri), i1 = __ldg(s.idx + 3 * tri + 1), i2 = __ldg(s.idx + 3 * tri + 2);
-    float3 a = vtx3(s.vtx, i0), b = vtx3(s.vtx, i1), c = vtx3(s.vtx, i2);
+    const float4* lr = s.lights + 4 * (size_t)li;
+    const float4 l0 = __ldg(lr), l1 = __ldg(lr + 1), l2 = __ldg(lr + 2), l3 = __ldg(lr + 3);
+    float3 a = f3(l0.x, l0.y, l0.z), b = f3(l1.x, l1.y, l1.z), c = f3(l2.x, l2.y, l2.z);
     // two uniforms in one call: the earlier dimension is the first argument
     float u1 = rnd_dim(r.seed, r.dim++);
     float u2 = rnd_dim(r.seed, r.dim++);
@@ -354,15 +367,14 @@ __device__ __forceinline__ bool sample_light(const DevScene& s, PathRegs& r, con
     float ct = dot(h.n, tl);
     float cl = -dot(ln, tl);
     if (!(ct > 0.0f && cl > 0.0f)) return false;
-    const wrk_material& lm = s.mats[__ldg(s.triMat + tri)];
     float pa = 1.0f / ((float)s.numEmissive * la);
     ls.lpdf = pa * d2 / fmaxf(cl, 1e-8f);
     ls.toLight = tl;
     ls.dist = dist;
     ls.d2 = d2;
     ls.cosTheta = ct;
-    ls.le = f3(lm.emission[0], lm.emission[1], lm.emission[2]);
-    ls.tri = tri;
+    ls.le = f3(l3.x, l3.y, l3.z);
+    ls.light = li;
     return true;
 }
 
@@ -373,7 +385,7 @@ struct ShadowOut {
     float3 o, d, c;
     float dist;
     uint32_t cont;
-    uint32_t lightTri;  // the light triangle the ray aims at
+    uint32_t light;     // the emissive-list entry of the light the ray aims at
     bool answered;      // the shadow query was answered here (the light blocks the ray)
 };
 
@@ -397,11 +409,12 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uin
     r.flags = st.w;
     uint32_t mat = __float_as_uint(h4.z);
     uint32_t prim = __float_as_uint(h4.y);
-    if (prim >= s.numTris) {
+    uint32_t leafPos = __float_as_uint(h4.w);
+    if (prim >= s.numTris || leafPos >= s.numTris) {
         atomicOr(f.err, kErrBadIndex);
         return kOutDone;
     }
-    HitAttr h = hit_program(s, r.o, r.d, h4.x, prim, mat);
+    HitAttr h = hit_program(s, r.o, r.d, h4.x, prim, mat, leafPos);
     const bool matOk = mat < s.numMats;
     // first-hit guides (trace.cu:267-286)
     if (r.flags & kFlagFirstHit) {
@@ -451,7 +464,7 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uin
                     so.d = ls.toLight;
                     so.dist = ls.dist;
                     so.c = con;
-                    so.lightTri = ls.tri;
+                    so.light = ls.light;
                     shadow = true;
                 }
             }
@@ -500,7 +513,7 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uin
             // answer (occluded) is known here, the shadow kernel has nothing to do,
             // and the path only continues, accumulates or ends.
             const Ray sr{so.o.x, so.o.y, so.o.z, so.d.x, so.d.y, so.d.z, kShadowTmin, so.dist - kShadowTmin};
-            if (so.lightTri < s.numTris && light_blocks(s, sr, so.lightTri)) {
+            if (so.light < s.numEmissive && light_blocks(s.lights + 4 * (size_t)so.light, sr)) {
                 so.answered = true;
                 if (so.cont == kContExt) return kOutCont;
                 if (so.cont == kContAccumulate) accumulate(f, r);

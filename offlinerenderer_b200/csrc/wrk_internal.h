@@ -88,6 +88,9 @@ struct DevScene {
     uint32_t numTex;
     const uint32_t* emissive;
     const float* cdf;
+    // per emissive entry (the order of emissive / cdf), 4 float4: v0 | triangle id,
+    // v1 | 0, v2 | 0, emission | 0 -- one 64-byte record per NEE light sample
+    const float4* lights;
     uint32_t numEmissive;
     uint32_t numTris;
     float env[3];

@@ -33,18 +33,15 @@ __device__ __forceinline__ bool mt_rn(const Ray& r, float4 a, float4 b, float4 c
     return true;
 }
 
-// Does the ray hit scene triangle `prim` within [tmin, tmax]?  The triangle record
-// is rebuilt from the scene's vertices exactly as the BVH builder writes it (v0,
-// v1 - v0, v2 - v0 with correctly rounded subtractions), so the answer is the one
-// the traversal's triangle test gives for the same triangle.
-__device__ __forceinline__ bool light_blocks(const DevScene& s, const Ray& r, uint32_t prim) {
-    const uint32_t i0 = __ldg(s.idx + 3 * prim), i1 = __ldg(s.idx + 3 * prim + 1), i2 = __ldg(s.idx + 3 * prim + 2);
-    const float ax = __ldg(s.vtx + 3 * i0), ay = __ldg(s.vtx + 3 * i0 + 1), az = __ldg(s.vtx + 3 * i0 + 2);
-    const float bx = __ldg(s.vtx + 3 * i1), by = __ldg(s.vtx + 3 * i1 + 1), bz = __ldg(s.vtx + 3 * i1 + 2);
-    const float cx = __ldg(s.vtx + 3 * i2), cy = __ldg(s.vtx + 3 * i2 + 1), cz = __ldg(s.vtx + 3 * i2 + 2);
-    const float4 a = make_float4(ax, ay, az, 0.0f);
-    const float4 b = make_float4(__fsub_rn(bx, ax), __fsub_rn(by, ay), __fsub_rn(bz, az), 0.0f);
-    const float4 c = make_float4(__fsub_rn(cx, ax), __fsub_rn(cy, ay), __fsub_rn(cz, az), 0.0f);
+// Does the ray hit the light triangle of light record `lr` (v0, v1, v2 in its first
+// three float4s) within [tmin, tmax]?  The triangle is rebuilt as the BVH builder
+// writes it (v0, v1 - v0, v2 - v0 with correctly rounded subtractions), so the
+// answer is the one the traversal's triangle test gives for the same triangle.
+__device__ __forceinline__ bool light_blocks(const float4* lr, const Ray& r) {
+    const float4 l0 = __ldg(lr), l1 = __ldg(lr + 1), l2 = __ldg(lr + 2);
+    const float4 a = make_float4(l0.x, l0.y, l0.z, 0.0f);
+    const float4 b = make_float4(__fsub_rn(l1.x, l0.x), __fsub_rn(l1.y, l0.y), __fsub_rn(l1.z, l0.z), 0.0f);
+    const float4 c = make_float4(__fsub_rn(l2.x, l0.x), __fsub_rn(l2.y, l0.y), __fsub_rn(l2.z, l0.z), 0.0f);
     float th;
     return mt_rn(r, a, b, c, th) && th >= r.tmin && th <= r.tmax;
 }
