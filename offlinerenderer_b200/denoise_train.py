@@ -1,6 +1,7 @@
 """Training of the learned denoiser, on the GPU end to end.
 
     python -m offlinerenderer_b200.denoise_train [--scenes 16] [--views 24] [--steps 12000] [--out PATH]
+    python -m offlinerenderer_b200.denoise_train --evaluate label=weights.wrkw [label=...]
     python -m torch.distributed.run --nproc-per-node N -m offlinerenderer_b200.denoise_train ...   (data parallel)
 
 The renderer itself generates the training pairs: seeded variants of the
@@ -156,6 +157,45 @@ def train(data, steps, batch=16, crop=128, lr=1e-3, seed=1, device=0, log=print,
     return dn, losses, time.time() - t0
 
 
+def evaluate(weights, size=256, spps=(1, 4, 16), ref_spp=4096, device=0, log=print) -> dict:
+    """Held-out quality of denoiser weights: the benchmark scene (scale test, seed 1,
+    never trained on) from its own camera and 3 orbit views, at `spps`; relMSE of the
+    denoised and of the noisy image against an FP64-accumulated ref_spp reference.
+    `weights` maps a label to a WRKUNET1 file; every file is scored on the same
+    renders."""
+    import torch
+
+    from . import quality
+
+    renderer = wrk.Renderer(device=device)
+    sd = scenes.scale_test(size, size, 4, seed=1)
+    scene = wrk.Scene.from_data(sd, device)
+    rng = np.random.default_rng(777)
+    cams = [scenes.Camera(position=sd.camera.position, target=sd.camera.target, up=sd.camera.up,
+                          fovY=sd.camera.fovY, aspect=1.0)] + [orbit_camera(rng, size, size) for _ in range(3)]
+    st0 = scenes.RenderSettings(size, size, 1, maxBounces=sd.settings.maxBounces,
+                                russianRouletteDepth=sd.settings.russianRouletteDepth, seed=sd.settings.seed)
+    dns = {}
+    for label, path in weights.items():
+        dns[label] = wrk.Denoiser(device=device)
+        load_weights(dns[label], path)
+    rows = []
+    for v, cam in enumerate(cams):
+        ref = quality.reference(renderer, scene, cam, st0, total_spp=ref_spp, chunk=512, device=device)
+        for s in spps:
+            rgb, alb, nrm, _ = quality.render(renderer, scene, cam, st0, s, 0, torch, device, True)
+            row = {"view": v, "spp": s, "noisy": quality.relmse(rgb, ref)}
+            for label, dn in dns.items():
+                out = torch.empty_like(rgb)
+                dn.infer_device(_Ptr(rgb), _Ptr(alb), _Ptr(nrm), 1, size, size, _Ptr(out))
+                row[label] = quality.relmse(out, ref)
+            rows.append(row)
+            log(json.dumps(row))
+    summary = {k: float(np.mean([r[k] for r in rows])) for k in ["noisy"] + list(weights)}
+    return {"views": len(cams), "size": size, "spps": list(spps), "reference_spp": ref_spp, "rows": rows,
+            "mean_relmse": summary}
+
+
 def write_weights(path: str, params: np.ndarray, meta: dict) -> None:
     """WRKUNET1 file: magic, u64 count, u64 metadata bytes, count bf16 bit patterns
     (the precision inference uses), JSON metadata.  wrk_denoiser_load reads it."""
@@ -198,7 +238,14 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--log", default=None)
+    ap.add_argument("--evaluate", nargs="*", default=None, metavar="LABEL=PATH",
+                    help="only score the given weights on the held-out benchmark scene and print JSON")
     args = ap.parse_args()
+    if args.evaluate is not None:
+        res = evaluate(dict(a.split("=", 1) for a in args.evaluate))
+        print(json.dumps(res["mean_relmse"]))
+        print(json.dumps(res))
+        return
     logf = open(args.log, "w") if args.log else None
 
     def log(msg):
