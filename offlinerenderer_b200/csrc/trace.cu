@@ -154,6 +154,11 @@ __device__ __forceinline__ void coop_set_ray(CoopLane& sm, const Ray& r, const f
     sm.tris[threadIdx.x] = tris;
 }
 
+__device__ __forceinline__ float3 ray_dir(const CoopLane& sm) {
+    const float4 d = sm.rayD[threadIdx.x];
+    return make_float3(d.x, d.y, d.z);
+}
+
 // Position of the k-th (0-based) set bit of m; k < popc(m).
 __device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t k) {
     uint32_t pos = 0;
@@ -553,10 +558,10 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
                 if constexpr (kMulti) {
                     const DevScene& sc = q.scenes[sceneIdx];
                     if (t.pBest != kNoHit) bucket = t.mBest < sc.numMats ? bucket_of(sc.mats[t.mBest].type) : kBucketOther;
-                    else miss_accumulate(sc, f, th, rd, make_float3(t.r.dx, t.r.dy, t.r.dz));
+                    else miss_accumulate(sc, f, th, rd, ray_dir(sm));
                 } else {
                     if (t.pBest != kNoHit) bucket = t.mBest < s0.numMats ? bucket_of(s0.mats[t.mBest].type) : kBucketOther;
-                    else miss_accumulate(s0, f, th, rd, make_float3(t.r.dx, t.r.dy, t.r.dz));
+                    else miss_accumulate(s0, f, th, rd, ray_dir(sm));
                 }
                 missed = t.pBest == kNoHit;
             }
@@ -569,8 +574,10 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
             }
             if (pos != kInvalidSlot) {
                 const PathQ o = pick_bucket(q, bucket);
-                o.ray_o[pos] = make_float4(t.r.ox, t.r.oy, t.r.oz, t.r.tmin);
-                o.ray_d[pos] = make_float4(t.r.dx, t.r.dy, t.r.dz, t.r.tmax);
+                // the ray as fetched, from the lane's shared-memory copy (the direction and
+                // tmax need no registers during traversal)
+                o.ray_o[pos] = sm.rayO[threadIdx.x];
+                o.ray_d[pos] = sm.rayD[threadIdx.x];
                 o.hit[pos] = make_float4(t.tBest, __uint_as_float(t.pBest), __uint_as_float(t.mBest),
                                          __uint_as_float(t.lBest));
                 o.thr[pos] = th;

@@ -55,12 +55,16 @@ def orbit_camera(rng, width: int, height: int, center=(0.5, 0.05, 0.5)) -> scene
 _Ptr = wrk.TensorPtr
 
 
-def render_views(scene, renderer, cams, size, spp, sample_offset, torch, device):
-    """Renders every camera at `spp` into (V, size, size, 3) rgb / albedo / normal tensors."""
+def render_views(scene, renderer, cams, size, spp, sample_offset, torch, device, out=None):
+    """Renders every camera at `spp` into (V, size, size, 3) rgb / albedo / normal tensors
+    (new ones, or the given `out` triple of views)."""
     V = len(cams)
-    rgb = torch.empty((V, size, size, 3), dtype=torch.float32, device=f"cuda:{device}")
-    alb = torch.empty_like(rgb)
-    nrm = torch.empty_like(rgb)
+    if out is None:
+        rgb = torch.empty((V, size, size, 3), dtype=torch.float32, device=f"cuda:{device}")
+        alb = torch.empty_like(rgb)
+        nrm = torch.empty_like(rgb)
+    else:
+        rgb, alb, nrm = out
     st = scene._data.settings
     st = scenes.RenderSettings(size, size, spp, maxBounces=st.maxBounces, russianRouletteDepth=st.russianRouletteDepth,
                                seed=st.seed, useNEE=st.useNEE)
@@ -71,33 +75,37 @@ def render_views(scene, renderer, cams, size, spp, sample_offset, torch, device)
 
 
 def generate(scene_seeds, views, size, target_spp, device=0, log=print):
-    """Renders the training set; returns a dict of device tensors."""
+    """Renders the training set straight into preallocated device tensors (views of
+    all scenes stacked); returns a dict: "target" -> (V, size, size, 3) and, per input
+    spp, (rgb, albedo, normal)."""
     import torch
 
     rng = np.random.default_rng(12345)
     renderer = wrk.Renderer(device=device)
-    tgt, inp = [], {k: ([], [], []) for k in INPUT_SPPS}
+    V = len(scene_seeds) * views
+    shape = (V, size, size, 3)
+    dev = f"cuda:{device}"
+    data = {"target": torch.empty(shape, dtype=torch.float32, device=dev)}
+    scratch = (torch.empty((views, size, size, 3), dtype=torch.float32, device=dev),
+               torch.empty((views, size, size, 3), dtype=torch.float32, device=dev))
+    for k in INPUT_SPPS:
+        data[k] = tuple(torch.empty(shape, dtype=torch.float32, device=dev) for _ in range(3))
     t0 = time.time()
-    for s in scene_seeds:
+    for j, s in enumerate(scene_seeds):
         sd = scenes.scale_test(size, size, 4, seed=s)
         scene = wrk.Scene.from_data(sd, device)
         cams = [scenes.Camera(position=sd.camera.position, target=sd.camera.target, up=sd.camera.up,
                               fovY=sd.camera.fovY, aspect=1.0)]
         cams += [orbit_camera(rng, size, size) for _ in range(views - 1)]
-        t, _, _ = render_views(scene, renderer, cams, size, target_spp, 0, torch, device)
-        tgt.append(t)
+        sl = slice(j * views, (j + 1) * views)
+        render_views(scene, renderer, cams, size, target_spp, 0, torch, device,
+                     out=(data["target"][sl], scratch[0], scratch[1]))
         off = target_spp
         for k in INPUT_SPPS:
-            r, a, n = render_views(scene, renderer, cams, size, k, off, torch, device)
+            render_views(scene, renderer, cams, size, k, off, torch, device, out=tuple(t[sl] for t in data[k]))
             off += k
-            inp[k][0].append(r)
-            inp[k][1].append(a)
-            inp[k][2].append(n)
         del scene
         log(f"scene seed {s}: {len(cams)} views rendered ({time.time() - t0:.1f} s)")
-    data = {"target": torch.cat(tgt)}
-    for k in INPUT_SPPS:
-        data[k] = tuple(torch.cat(x) for x in inp[k])
     torch.cuda.synchronize()
     return data
 

@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 from conftest import GOLDEN
+from level1 import BSDF_COLS, COND, TOL, _rel, check_against_fp64
 from offlinerenderer_b200 import scenes
 
 pytestmark = pytest.mark.gpu
@@ -81,50 +82,6 @@ def test_compaction_bitexact(gpu, oracle):
     assert len(gpu.compact(stage, np.arange(5000, dtype=np.uint32))) == 0
 
 
-# Level-1 bound (north star): every finite BSDF / sampling / MIS output within 1e-5
-# relative of the FP64 transcription of the reference's formulas.  Records are left
-# out only by a computed condition criterion: where the reference's OWN FP32
-# arithmetic (the oracle's FP32 port, bit-identical to the reference build compiled
-# on the host) already differs from FP64 by more than half the tolerance, the
-# quantity is ill-conditioned in FP32 at that input -- e.g. the GGX D term near its
-# peak at low roughness, where 1 - NoH^2 (1 - a^2) cancels and amplifies the
-# rounding of NoH by ~1/a^2 -- and no FP32 evaluation of the same formula can be
-# held to 1e-5 there.  The excluded fraction is capped per column below (measured
-# on these seeded inputs; roughness U(0.05, 1)).
-TOL = 1e-5
-COND = 0.5 * TOL
-BSDF_COLS = [c for c in range(34) if c not in (8, 16)]  # 8, 16: integer outputs
-# per-column cap on the excluded fraction: the VNDF sample pdf (7) is the D term at
-# the sampled half-vector, ill-conditioned for roughness below ~0.3
-EXCLUDE_CAP = {7: 0.30}
-EXCLUDE_CAP_DEFAULT = 0.02
-
-
-def _rel(x, r):
-    with np.errstate(divide="ignore", invalid="ignore"):
-        d = np.abs(x - r) / np.abs(r)
-    d[(r == 0) & (x == 0)] = 0.0
-    d[(r == 0) & (x != 0)] = np.inf
-    return d
-
-
-def _check_against_fp64(g, o32, o64, label):
-    """Max relative error of g vs o64 over the well-conditioned finite records of
-    every column; returns {column: (max error, excluded fraction)}."""
-    report = {}
-    for c in BSDF_COLS:
-        fin = np.isfinite(o64[:, c]) & np.isfinite(o32[:, c])
-        # non-finite where the reference is non-finite (e.g. the 0/0 pdf of A14), nowhere else
-        assert np.array_equal(np.isfinite(g[:, c]), fin), (label, c)
-        cond = fin & (_rel(o32[:, c], o64[:, c]) <= COND)
-        excluded = 1.0 - cond.sum() / max(1, fin.sum())
-        assert excluded <= EXCLUDE_CAP.get(c, EXCLUDE_CAP_DEFAULT), (label, c, excluded)
-        err = float(_rel(g[cond, c], o64[cond, c]).max()) if cond.any() else 0.0
-        report[c] = (err, excluded)
-        assert err < TOL, (label, c, err, excluded)
-    return report
-
-
 def test_bsdf_fp32_vs_oracle(gpu, oracle):
     """The device's FP32 shading math against the oracle's FP32 restatement (the
     reference's expression order, correctly rounded operations): integer outputs
@@ -154,7 +111,7 @@ def test_bsdf_vs_fp64_transcription(gpu, oracle):
 
     inp = pyoracle.random_bsdf_inputs(100000, seed=12)
     g = gpu.bsdf_batch(inp).astype(np.float64)
-    report = _check_against_fp64(g, oracle.bsdf(inp, 0), oracle.bsdf(inp, 1), "random")
+    report = check_against_fp64(g, oracle.bsdf(inp, 0), oracle.bsdf(inp, 1), "random")
     worst = max(report.values())
     print("level-1 max rel error vs FP64 over well-conditioned records:", worst)
 
@@ -166,7 +123,7 @@ def test_golden_bsdf_fixture(gpu, oracle):
     g = gpu.bsdf_batch(d["inputs"]).astype(np.float64)
     o = d["outputs"]
     assert np.array_equal(g[:, 8], o[:, 8]) and np.array_equal(g[:, 16], o[:, 16])
-    _check_against_fp64(g, o, oracle.bsdf(d["inputs"], 1), "golden")
+    check_against_fp64(g, o, oracle.bsdf(d["inputs"], 1), "golden")
 
 
 def test_camera_rays_bitexact(gpu, oracle):

@@ -116,6 +116,71 @@ def test_light_cdf_restatement(oracle):
     assert cdf[0] == np.float32(0.5)
 
 
+def _light_cdf_numpy(sd):
+    """scene.cpp:423-491 restated in numpy float32, independently of the oracle: per
+    emissive triangle in index order, power = (ex + ey + ez) * area with area =
+    0.5 * |cross(v1 - v0, v2 - v0)| (correctly rounded float32 steps, left to right),
+    a serial float32 prefix sum, then each entry divided by the total."""
+    f = np.float32
+    tris, cdf, total = [], [], f(0.0)
+    for t in range(sd.num_triangles):
+        m = sd.materials[sd.tri_material[t]]
+        if m["type"] != scenes.EMISSIVE:
+            continue
+        a, b, c = (sd.vertices[sd.indices[t][k]].astype(np.float32) for k in range(3))
+        e1, e2 = b - a, c - a
+        cr = np.array([e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                       e1[0] * e2[1] - e1[1] * e2[0]], np.float32)
+        area = f(0.5) * np.sqrt(f(f(cr[0] * cr[0] + cr[1] * cr[1]) + cr[2] * cr[2]))
+        em = m["emission"]
+        power = f(f(em[0] + em[1]) + em[2]) * area
+        total = f(total + power)
+        tris.append(t)
+        cdf.append(total)
+    return np.array(tris, np.uint32), (np.array(cdf, np.float32) / total).astype(np.float32)
+
+
+def test_light_cdf_scale_scene_matches_numpy_restatement(oracle):
+    """The 64 lights of unequal power of the scale scene: the oracle's light list and
+    CDF equal the numpy restatement bit for bit (the GPU tests then compare the
+    product's CDF with the oracle's)."""
+    sd = scenes.scale_test(48, 32, 1, seed=1)
+    tris, cdf = oracle.scene(sd).light_cdf()
+    want_t, want_c = _light_cdf_numpy(sd)
+    assert len(tris) == 64
+    assert np.array_equal(tris, want_t)
+    assert np.array_equal(cdf.view(np.uint32), want_c.view(np.uint32))
+
+
+@pytest.mark.parametrize("full", [False, True])
+def test_fp64_bvh_walk_equals_all_triangle_test(oracle, full):
+    """Oracle mode 2 (the FP64 test on the triangles a widened FP64 BVH walk reaches)
+    returns exactly what mode 1 (FP64 over every triangle) returns: on a small scale
+    scene for 4000 rays, and on the full 2.41M-triangle scale scene for a sample."""
+    from test_gpu_trace import camera_like_rays, random_rays
+
+    sd = scenes.scale_test(1920, 1080, 1, seed=1) if full else \
+        scenes.scale_test(64, 36, 1, grid=96, spheres=30, lights=16, seed=2)
+    n = 24 if full else 2000
+    rays = np.concatenate([camera_like_rays(oracle, sd, n, 21), random_rays(sd, n, 22)])
+    osc = oracle.scene(sd)
+    t1, p1 = osc.closest(rays, mode=1)
+    t2, p2 = osc.closest(rays, mode=2)
+    assert np.array_equal(p1, p2) and np.array_equal(t1, t2)
+    assert (p1 != 0xFFFFFFFF).sum() > n // 4
+
+
+def test_level1_caps_hold_for_the_reference_build(oracle):
+    """The level-1 criterion and its exclusion caps, applied to the reference's own
+    FP32 outputs (the golden fixture from the reference build): every
+    well-conditioned output of the reference is within 1e-5 of the FP64
+    transcription (so the GPU test's bound is met by the reference itself)."""
+    from level1 import check_against_fp64
+
+    d = np.load(os.path.join(GOLDEN, "bsdf_ref.npz"))
+    check_against_fp64(d["outputs"], d["outputs"], oracle.bsdf(d["inputs"], 1), "reference")
+
+
 def test_iteration_cap_drops_paths(oracle):
     """maxIterations bounds the wavefront iterations; fewer iterations can only
     drop energy (paths still alive at the cap are not accumulated)."""
