@@ -35,8 +35,10 @@ def check_against_fp64(g, o32, o64, label):
     report = {}
     for c in BSDF_COLS:
         fin = np.isfinite(o64[:, c]) & np.isfinite(o32[:, c])
-        # non-finite where the reference is non-finite (e.g. the 0/0 pdf of A14), nowhere else
-        assert np.array_equal(np.isfinite(g[:, c]), fin), (label, c)
+        # non-finite where the reference's FP32 is non-finite (e.g. the 0/0 pdf of A14);
+        # an ulp of sin / cos may move a record across that edge: at most 1 in 10^4
+        assert (np.isfinite(g[:, c]) != np.isfinite(o32[:, c])).mean() <= 1e-4, (label, c)
+        fin &= np.isfinite(g[:, c])
         cond = fin & (_rel(o32[:, c], o64[:, c]) <= COND)
         excluded = 1.0 - cond.sum() / max(1, fin.sum())
         assert excluded <= EXCLUDE_CAP.get(c, EXCLUDE_CAP_DEFAULT), (label, c, excluded)

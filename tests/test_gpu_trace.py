@@ -66,9 +66,11 @@ def _check_level2(t, p, t64, p64):
     miss = np.uint32(0xFFFFFFFF)
     agree = (p == p64).mean()
     assert agree >= 0.9999, agree
-    both = (p != miss) & (p64 != miss)
     assert ((p != miss) == (p64 != miss)).mean() >= 0.9999
-    rel = np.abs(t[both].astype(np.float64) - t64[both]) / np.abs(t64[both])
+    # t of every ray whose primitive agrees (a ray that grazes a silhouette may hit
+    # another surface in FP32 than in FP64: that is a primitive disagreement)
+    hit = (p == p64) & (p != miss)
+    rel = np.abs(t[hit].astype(np.float64) - t64[hit]) / np.abs(t64[hit])
     assert rel.max() < 1e-5, rel.max()
     return agree
 
