@@ -153,7 +153,10 @@ int wrk_scene_set_environment_map(wrk_scene* s, const float* rgba, uint32_t widt
  * (replaces optixAccelBuild, scene.cpp:493-550). */
 int wrk_scene_finalize(wrk_scene* s);
 int wrk_scene_bvh_info(wrk_scene* s, wrk_bvh_info* info);
-/* Light list / CDF readback (getEmissiveTrianglesBuffer, getEmissiveTriangleCDFBuffer). */
+/* Light list / CDF readback (getEmissiveTrianglesBuffer, getEmissiveTriangleCDFBuffer):
+ * the emissive triangle ids and their power CDF as the device holds them; *count
+ * receives the number of entries.  With tris and cdf both NULL this is a size query;
+ * otherwise capacity below the count is WRK_ERR_INVALID. */
 int wrk_scene_light_cdf(wrk_scene* s, uint32_t* tris, float* cdf, uint32_t capacity, uint32_t* count);
 
 /* Copies the 8-wide BVH to host memory for inspection: nodes = numNodes * 20 u32

@@ -630,6 +630,7 @@ int wrk_scene_light_cdf(wrk_scene* s, uint32_t* tris, float* cdf, uint32_t capac
     if (rc) return rc;
     uint32_t n = (uint32_t)s->emissive.size();
     if (count) *count = n;
+    if (!tris && !cdf) return WRK_OK;  // size query
     if (n > capacity) return fail(WRK_ERR_INVALID, "capacity %u < %u emissive triangles", capacity, n);
     if (n) {
         // read back what the device holds

@@ -128,128 +128,6 @@ struct Trav {
     uint32_t lBest;  // leaf position (index into the BVH triangle records) of the best hit
 };
 
-// Warp-cooperative triangle tests.  After a node step every lane may hold a run of
-// triangles (tBase + the set bits of tMask); instead of each lane looping over its
-// own (a warp then waits for its longest leaf, ~23 % lane occupancy), the warp
-// numbers all pending (lane, triangle) jobs with a prefix sum and tests them 32 at a
-// time, each lane taking one job of any owner.  A job reads its owner's ray from
-// shared memory and merges its hit into the owner's best with one 64-bit shared
-// atomicMin on (t bits << 32 | prim): t >= tmin >= 0 orders like its bits, so the
-// minimum is the nearest hit with ties going to the lower primitive id -- the same
-// result as the sequential loop, whatever order the jobs run in.
-struct CoopLane {
-    float4 rayO[kTraceBlock];           // owner's ray: origin | tmin
-    float4 rayD[kTraceBlock];           //              direction | tmax
-    uint4 job[kTraceBlock];             // owner's tBase, tMask, first job index, numTris
-    unsigned long long key[kTraceBlock];  // owner's best (t bits << 32 | prim)
-    const float4* tris[kTraceBlock];    // owner's triangle records (scene of its ray)
-    uint32_t mat[kTraceBlock];          // material of the owner's best hit
-    uint32_t pos[kTraceBlock];          // its leaf position
-    uint8_t startLane[kTraceBlock];     // per warp: lane whose jobs start at window slot p
-};
-
-__device__ __forceinline__ void coop_set_ray(CoopLane& sm, const Ray& r, const float4* tris) {
-    sm.rayO[threadIdx.x] = make_float4(r.ox, r.oy, r.oz, r.tmin);
-    sm.rayD[threadIdx.x] = make_float4(r.dx, r.dy, r.dz, r.tmax);
-    sm.tris[threadIdx.x] = tris;
-}
-
-__device__ __forceinline__ float3 ray_dir(const CoopLane& sm) {
-    const float4 d = sm.rayD[threadIdx.x];
-    return make_float3(d.x, d.y, d.z);
-}
-
-// Position of the k-th (0-based) set bit of m; k < popc(m).
-__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t k) {
-    uint32_t pos = 0;
-#pragma unroll
-    for (uint32_t w = 16; w; w >>= 1) {
-        const uint32_t c = __popc(m & ((1u << w) - 1u));
-        if (k >= c) {
-            k -= c;
-            m >>= w;
-            pos += w;
-        }
-    }
-    return pos;
-}
-
-// Tests every lane's pending triangles (t.tMask relative to t.tBase) cooperatively;
-// called by all 32 lanes of the warp together (lanes without triangles have tMask 0).
-__device__ __forceinline__ void coop_triangles(Trav& t, uint32_t numTris, CoopLane& sm, uint32_t* errFlag) {
-    const uint32_t lane = threadIdx.x & 31u, wbase = threadIdx.x & ~31u;
-    const uint32_t cnt = __popc(t.tMask);
-    uint32_t incl = cnt;
-#pragma unroll
-    for (uint32_t o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-    }
-    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    if (total == 0) return;
-    const uint32_t excl = incl - cnt;
-    if (cnt) {
-        sm.job[threadIdx.x] = make_uint4(t.tBase, t.tMask, excl, numTris);
-        sm.key[threadIdx.x] = ((unsigned long long)__float_as_uint(t.tBest) << 32) | t.pBest;
-    }
-    for (uint32_t base = 0; base < total; base += 32) {
-        // lanes whose job run starts in this window, and the one running into it
-        const bool startsHere = cnt && excl >= base && excl < base + 32u;
-        if (startsHere) sm.startLane[wbase + (excl - base)] = (uint8_t)lane;
-        const uint32_t starts = __reduce_or_sync(0xffffffffu, startsHere ? 1u << (excl - base) : 0u);
-        const uint32_t span = __ballot_sync(0xffffffffu, cnt && excl < base && incl > base);
-        __syncwarp();
-        const uint32_t j = base + lane;
-        bool hit = false;
-        uint32_t owner = 0;
-        unsigned long long key = 0;
-        uint32_t mat = 0, tri = 0;
-        if (j < total) {
-            const uint32_t below = starts & (lane == 31u ? 0xffffffffu : ((2u << lane) - 1u));
-            // every job has an owner (a run starting in the window at or before it, or
-            // the one run entering the window); the mask keeps the index in the warp
-            owner = (below ? sm.startLane[wbase + 31u - __clz(below)] : (uint32_t)(__ffs(span) - 1)) & 31u;
-            const uint4 jb = sm.job[wbase + owner];
-            tri = jb.x + nth_set_bit(jb.y, j - jb.z);
-            if (tri >= jb.w) {
-                atomicOr(errFlag, kErrBadIndex);
-            } else {
-                const float4* tp = sm.tris[wbase + owner] + 3 * (size_t)tri;
-                const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-                const float4 o = sm.rayO[wbase + owner], d = sm.rayD[wbase + owner];
-                const Ray r{o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w};
-                float th;
-                if (mt_rn(r, a, b, c, th) && th >= r.tmin && th <= r.tmax) {
-                    // th + 0 turns a -0 hit distance into +0 so its bits order correctly
-                    key = ((unsigned long long)__float_as_uint(__fadd_rn(th, 0.0f)) << 32) | __float_as_uint(a.w);
-                    mat = __float_as_uint(b.w);
-                    hit = true;
-                    atomicMin(&sm.key[wbase + owner], key);
-                }
-            }
-        }
-        __syncwarp();
-        // the job that holds its owner's minimum records the material and leaf position
-        if (hit && sm.key[wbase + owner] == key) {
-            sm.mat[wbase + owner] = mat;
-            sm.pos[wbase + owner] = tri;
-        }
-        __syncwarp();
-    }
-    if (cnt) {
-        const unsigned long long key = sm.key[threadIdx.x];
-        const float tb = __uint_as_float((uint32_t)(key >> 32));
-        const uint32_t pb = (uint32_t)key;
-        if (pb != t.pBest || tb != t.tBest) {
-            t.tBest = tb;
-            t.pBest = pb;
-            t.mBest = sm.mat[threadIdx.x];
-            t.lBest = sm.pos[threadIdx.x];
-        }
-        t.tMask = 0;
-    }
-}
-
 __device__ __forceinline__ void trav_init(Trav& t, const Ray& r) {
     t.r = r;
     // Direction components below 2^-80 in magnitude are replaced by +-2^-80 for
@@ -275,65 +153,88 @@ __device__ __forceinline__ void trav_init(Trav& t, const Ray& r) {
     t.lBest = 0;
 }
 
-// One traversal step of the warp, called by all 32 lanes together; `part` lanes
-// have a ray in flight.  Each such lane descends into the next child of its current
-// node group (pushing the group's remainder) and picks up the triangles that node
-// exposes; the warp tests all of them cooperatively; then a lane whose group is used
-// up pops the next one.  Returns true for a lane whose ray is finished (closest hit:
-// stack empty; any hit: a hit found; or an internal error).  Closest hit keeps ties
-// in t with the lower primitive index.
+// One traversal step: descend into the next child of the current node group
+// (pushing the group's remainder), test the triangles that node exposes, and pop
+// when the group is used up.  Returns true when the ray is finished.  Closest hit
+// keeps ties in t with the lower primitive index; any hit stops at the first hit.
 template <bool kAnyHit, class Geom>
-__device__ __forceinline__ bool trav_step(const Geom& s, Trav& t, bool part, uint2* sstack, uint2* lstack,
-                                          CoopLane& sm, uint32_t* errFlag) {
+__device__ __forceinline__ bool trav_step(const Geom& s, Trav& t, uint2* sstack, uint2* lstack,
+                                          uint32_t* errFlag) {
     const int tid = threadIdx.x;
-    bool fin = false;
-    if (part) {
-        if (++t.visits > kMaxVisits) {  // a malformed tree must not spin forever
+    if (++t.visits > kMaxVisits) {  // a malformed tree must not spin forever
+        atomicOr(errFlag, kErrBadIndex);
+        return true;
+    }
+    if (t.gHits) {
+        uint32_t pos = __ffs(t.gHits) - 1;
+        t.gHits &= t.gHits - 1;
+        uint32_t slot = pos ^ t.octInv;
+        uint32_t child = t.gBase + __popc(t.gImask & ((1u << slot) - 1u));
+        if (t.gHits) {
+            uint2 e = make_uint2(t.gBase, t.gHits | (t.gImask << 8));
+            if (t.sp < kStackSmem) sstack[t.sp * kTraceBlock + tid] = e;
+            else if (t.sp < kStackSmem + kStackLocal) lstack[t.sp - kStackSmem] = e;
+            else {
+                atomicOr(errFlag, kErrStackOverflow);
+                return true;
+            }
+            ++t.sp;
+        }
+        if (child >= s.numNodes) {
             atomicOr(errFlag, kErrBadIndex);
-            fin = true;
-        } else if (t.gHits) {
-            uint32_t pos = __ffs(t.gHits) - 1;
-            t.gHits &= t.gHits - 1;
-            uint32_t slot = pos ^ t.octInv;
-            uint32_t child = t.gBase + __popc(t.gImask & ((1u << slot) - 1u));
-            if (t.gHits) {
-                uint2 e = make_uint2(t.gBase, t.gHits | (t.gImask << 8));
-                if (t.sp < kStackSmem) sstack[t.sp * kTraceBlock + tid] = e;
-                else if (t.sp < kStackSmem + kStackLocal) lstack[t.sp - kStackSmem] = e;
-                else {
-                    atomicOr(errFlag, kErrStackOverflow);
-                    fin = true;
-                }
-                ++t.sp;
+            return true;
+        }
+        intersect_node(s.nodes, child, t.r, t.ix, t.iy, t.iz, t.octInv, t.tBest, t.gBase, t.tBase, t.gHits, t.gImask,
+                       t.tMask);
+        if (t.tMask && t.tBase + (31u - __clz(t.tMask)) >= s.numTris) {
+            atomicOr(errFlag, kErrBadIndex);
+            return true;
+        }
+    }
+    while (t.tMask) {
+        uint32_t j = __ffs(t.tMask) - 1;
+        t.tMask &= t.tMask - 1;
+        const float4* tp = s.tris + 3 * (size_t)(t.tBase + j);
+        float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+        float th;
+        if (mt_rn(t.r, a, b, c, th) && th >= t.r.tmin && th <= t.r.tmax) {
+            uint32_t prim = __float_as_uint(a.w);
+            if (kAnyHit) {
+                t.tBest = th;
+                t.pBest = prim;
+                return true;
             }
-            if (!fin && child >= s.numNodes) {
-                atomicOr(errFlag, kErrBadIndex);
-                fin = true;
-            }
-            if (!fin) {
-                intersect_node(s.nodes, child, t.r, t.ix, t.iy, t.iz, t.octInv, t.tBest, t.gBase, t.tBase, t.gHits,
-                               t.gImask, t.tMask);
-                if (t.tMask && t.tBase + (31u - __clz(t.tMask)) >= s.numTris) {
-                    atomicOr(errFlag, kErrBadIndex);
-                    fin = true;
-                }
+            if (th < t.tBest || (th == t.tBest && prim < t.pBest)) {
+                t.tBest = th;
+                t.pBest = prim;
+                t.mBest = __float_as_uint(b.w);
+                t.lBest = t.tBase + j;
             }
         }
     }
-    if (!part || fin) t.tMask = 0;
-    coop_triangles(t, s.numTris, sm, errFlag);
-    if (part && !fin) {
-        if (kAnyHit && t.pBest != kNoHit) return true;
-        if (!t.gHits) {
-            if (t.sp == 0) return true;
-            --t.sp;
-            uint2 e = t.sp < kStackSmem ? sstack[t.sp * kTraceBlock + tid] : lstack[t.sp - kStackSmem];
-            t.gBase = e.x;
-            t.gHits = e.y & 0xffu;
-            t.gImask = e.y >> 8;
-        }
+    if (!t.gHits) {
+        if (t.sp == 0) return true;
+        --t.sp;
+        uint2 e = t.sp < kStackSmem ? sstack[t.sp * kTraceBlock + tid] : lstack[t.sp - kStackSmem];
+        t.gBase = e.x;
+        t.gHits = e.y & 0xffu;
+        t.gImask = e.y >> 8;
     }
-    return fin;
+    return false;
+}
+
+template <bool kAnyHit>
+__device__ __forceinline__ bool traverse(const DevScene& s, const Ray& r, float& tBest, uint32_t& pBest,
+                                         uint32_t& mBest, uint2* sstack, uint32_t* errFlag) {
+    uint2 lstack[kStackLocal];
+    Trav t;
+    trav_init(t, r);
+    while (!trav_step<kAnyHit>(s, t, sstack, lstack, errFlag)) {
+    }
+    tBest = t.tBest;
+    pBest = t.pBest;
+    mBest = t.mBest;
+    return t.pBest != kNoHit;
 }
 
 __device__ __forceinline__ Ray load_ray8(const float* p) {
@@ -342,40 +243,28 @@ __device__ __forceinline__ Ray load_ray8(const float* p) {
     return Ray{a.x, a.y, a.z, b.x, b.y, b.z, a.w, b.w};
 }
 
-// One ray per thread; the warp steps together (cooperative triangle tests), lanes
-// past n take part without a ray.
-template <bool kAnyHit>
-__device__ __forceinline__ void query_rays(const DevScene& s, const float* __restrict__ rays, uint32_t n, float* tOut,
-                                           uint32_t* pOut, uint32_t* occ, uint32_t* err) {
-    __shared__ uint2 sstack[kStackSmem * kTraceBlock];
-    __shared__ CoopLane sm;
-    uint2 lstack[kStackLocal];
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool have = i < n;
-    Trav t;
-    trav_init(t, have ? load_ray8(rays + 8 * (size_t)i) : Ray{0, 0, 0, 1, 0, 0, 0, -1});
-    coop_set_ray(sm, t.r, s.tris);
-    TraceGeom geo{s.nodes, s.tris, s.numNodes, s.numTris};
-    bool fin = !have;
-    while (__any_sync(0xffffffffu, !fin)) fin |= trav_step<kAnyHit>(geo, t, !fin, sstack, lstack, sm, err);
-    if (!have) return;
-    const bool hit = t.pBest != kNoHit;
-    if (kAnyHit) {
-        occ[i] = hit ? 1u : 0u;
-    } else {
-        tOut[i] = hit ? t.tBest : __int_as_float(0x7f800000);
-        pOut[i] = hit ? t.pBest : kNoHit;
-    }
-}
-
 __global__ void __launch_bounds__(kTraceBlock) k_closest_query(DevScene s, const float* __restrict__ rays, uint32_t n,
                                                                float* tOut, uint32_t* pOut, uint32_t* err) {
-    query_rays<false>(s, rays, n, tOut, pOut, nullptr, err);
+    __shared__ uint2 sstack[kStackSmem * kTraceBlock];
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Ray r = load_ray8(rays + 8 * (size_t)i);
+    float t;
+    uint32_t p, m;
+    bool hit = traverse<false>(s, r, t, p, m, sstack, err);
+    tOut[i] = hit ? t : __int_as_float(0x7f800000);
+    pOut[i] = hit ? p : kNoHit;
 }
 
 __global__ void __launch_bounds__(kTraceBlock) k_occluded_query(DevScene s, const float* __restrict__ rays,
                                                                 uint32_t n, uint32_t* out, uint32_t* err) {
-    query_rays<true>(s, rays, n, nullptr, nullptr, out, err);
+    __shared__ uint2 sstack[kStackSmem * kTraceBlock];
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Ray r = load_ray8(rays + 8 * (size_t)i);
+    float t;
+    uint32_t p, m;
+    out[i] = traverse<true>(s, r, t, p, m, sstack, err) ? 1u : 0u;
 }
 
 void launch_closest_query(const DevScene& s, const float* rays, uint32_t n, float* t, uint32_t* prim, uint32_t* err,
@@ -466,7 +355,6 @@ __device__ __forceinline__ void count_ended_t(SlotCtl* ctl, bool ended, uint32_t
 template <bool kAnyHit, bool kMulti>
 __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_persistent(DevScene s0, Queues q) {
     __shared__ uint2 sstack[kStackSmem * kTraceBlock];
-    __shared__ CoopLane sm;
     uint2 lstack[kStackLocal];
     Counters* c = q.ctr;
     const uint32_t cur = c->cur;
@@ -501,7 +389,6 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
                         geo = TraceGeom{sc.nodes, sc.tris, sc.numNodes, sc.numTris};
                     }
                     trav_init(t, Ray{o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w});
-                    coop_set_ray(sm, t.r, geo.tris);
                     active = true;
                 } else {
                     exhausted = true;
@@ -513,7 +400,7 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
         const int refillAt = __any_sync(0xffffffffu, exhausted) ? 1 : kRefillAt;
         bool fin = false;
         do {
-            fin |= trav_step<kAnyHit>(geo, t, active && !fin, sstack, lstack, sm, &c->error);
+            if (active && !fin) fin = trav_step<kAnyHit>(geo, t, sstack, lstack, &c->error);
         } while (__popc(__ballot_sync(0xffffffffu, active && !fin)) >= refillAt);
         const bool done = active && fin;
         if (kAnyHit) {
@@ -558,10 +445,10 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
                 if constexpr (kMulti) {
                     const DevScene& sc = q.scenes[sceneIdx];
                     if (t.pBest != kNoHit) bucket = t.mBest < sc.numMats ? bucket_of(sc.mats[t.mBest].type) : kBucketOther;
-                    else miss_accumulate(sc, f, th, rd, ray_dir(sm));
+                    else miss_accumulate(sc, f, th, rd, make_float3(t.r.dx, t.r.dy, t.r.dz));
                 } else {
                     if (t.pBest != kNoHit) bucket = t.mBest < s0.numMats ? bucket_of(s0.mats[t.mBest].type) : kBucketOther;
-                    else miss_accumulate(s0, f, th, rd, ray_dir(sm));
+                    else miss_accumulate(s0, f, th, rd, make_float3(t.r.dx, t.r.dy, t.r.dz));
                 }
                 missed = t.pBest == kNoHit;
             }
@@ -574,10 +461,8 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
             }
             if (pos != kInvalidSlot) {
                 const PathQ o = pick_bucket(q, bucket);
-                // the ray as fetched, from the lane's shared-memory copy (the direction and
-                // tmax need no registers during traversal)
-                o.ray_o[pos] = sm.rayO[threadIdx.x];
-                o.ray_d[pos] = sm.rayD[threadIdx.x];
+                o.ray_o[pos] = make_float4(t.r.ox, t.r.oy, t.r.oz, t.r.tmin);
+                o.ray_d[pos] = make_float4(t.r.dx, t.r.dy, t.r.dz, t.r.tmax);
                 o.hit[pos] = make_float4(t.tBest, __uint_as_float(t.pBest), __uint_as_float(t.mBest),
                                          __uint_as_float(t.lBest));
                 o.thr[pos] = th;

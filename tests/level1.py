@@ -1,37 +1,89 @@
-"""The level-1 bound shared by the GPU kernel tests and the CPU check of the
-reference's own FP32 outputs (see the comment below)."""
+"""The level-1 bound (north star): every finite BSDF / sampling / MIS output within
+1e-5 relative of the FP64 transcription of the reference's formulas.  Shared by the
+GPU kernel tests and the CPU check of the reference's own FP32 outputs.
+
+Error metric.  Scalar outputs (eval, pdf, Fresnel, MIS weight, area, correction)
+are compared relative to their own magnitude.  Vector outputs -- the VNDF and
+cosine sample directions, the tangent frame, the sampled light point and its
+normal -- are compared relative to the vector's length: a unit direction's
+component near zero has no meaningful relative precision of its own.
+
+Condition criterion.  A record is left out of an output's bound only where that
+output is ill-conditioned in FP32 there: where the reference's OWN FP32
+arithmetic (the oracle's FP32 port, bit-identical to the reference build
+compiled on the host) differs from FP64 by more than half the tolerance, at the
+record or at any of four neighbouring records whose random numbers u0..u2 are
+one float32 ulp away.  The neighbours matter because FP32 rounding error near an
+ill-conditioned point is erratic -- one evaluation may land close to FP64 by
+chance -- and because a one-ulp change of a random number moves the sampling
+angle by as much as the one- or two-ulp differences between CUDA's and glibc's
+sin / cos.  Example: the GGX D term near its peak at low roughness, where
+1 - NoH^2 (1 - a^2) cancels and multiplies the rounding of NoH by about 1/a^2.
+The excluded fraction is capped per column (measured on the seeded inputs;
+roughness U(0.05, 1)).
+"""
 import numpy as np
 
-# Level-1 bound (north star): every finite BSDF / sampling / MIS output within 1e-5
-# relative of the FP64 transcription of the reference's formulas.  Records are left
-# out only by a computed condition criterion: where the reference's OWN FP32
-# arithmetic (the oracle's FP32 port, bit-identical to the reference build compiled
-# on the host) already differs from FP64 by more than half the tolerance, the
-# quantity is ill-conditioned in FP32 at that input -- e.g. the GGX D term near its
-# peak at low roughness, where 1 - NoH^2 (1 - a^2) cancels and amplifies the
-# rounding of NoH by ~1/a^2 -- and no FP32 evaluation of the same formula can be
-# held to 1e-5 there.  The excluded fraction is capped per column below (measured
-# on these seeded inputs; roughness U(0.05, 1)).
 TOL = 1e-5
 COND = 0.5 * TOL
 BSDF_COLS = [c for c in range(34) if c not in (8, 16)]  # 8, 16: integer outputs
+# outputs that are 3-vectors: VNDF sample direction, cosine sample direction,
+# tangent, bitangent, sampled light point, light normal
+VEC_GROUPS = [(4, 5, 6), (10, 11, 12), (20, 21, 22), (23, 24, 25), (26, 27, 28), (30, 31, 32)]
 # per-column cap on the excluded fraction: the VNDF sample pdf (7) is the D term at
 # the sampled half-vector, ill-conditioned for roughness below ~0.3
-EXCLUDE_CAP = {7: 0.30}
-EXCLUDE_CAP_DEFAULT = 0.02
+EXCLUDE_CAP = {7: 0.35}
+EXCLUDE_CAP_DEFAULT = 0.03
+U_COLS = slice(15, 18)  # the record's random numbers u0, u1, u2
 
 
-def _rel(x, r):
+def scale_of(r):
+    """|r| per entry, the vector length for the columns of VEC_GROUPS."""
+    s = np.abs(r).astype(np.float64)
+    for g in VEC_GROUPS:
+        v = r[:, list(g)].astype(np.float64)
+        n = np.sqrt(np.nansum(v * v, axis=1))
+        for c in g:
+            s[:, c] = n
+    return s
+
+
+def rel_err(x, r):
+    """|x - r| / scale_of(r); 0 where both are 0, inf where only r is 0."""
+    s = scale_of(r)
     with np.errstate(divide="ignore", invalid="ignore"):
-        d = np.abs(x - r) / np.abs(r)
-    d[(r == 0) & (x == 0)] = 0.0
-    d[(r == 0) & (x != 0)] = np.inf
+        d = np.abs(x.astype(np.float64) - r) / s
+    d[(s == 0) & (x == r)] = 0.0
+    d[(s == 0) & (x != r)] = np.inf
     return d
 
 
-def check_against_fp64(g, o32, o64, label):
-    """Max relative error of g vs o64 over the well-conditioned finite records of
-    every column; returns {column: (max error, excluded fraction)}."""
+def neighbour(inp, seed):
+    """The records with u0..u2 each moved one float32 ulp up or down (random signs)."""
+    rng = np.random.default_rng(seed)
+    out = np.array(inp, np.float32, copy=True)
+    u = out[:, U_COLS]
+    up = rng.random(u.shape) < 0.5
+    out[:, U_COLS] = np.where(up, np.nextafter(u, np.float32(2.0)), np.nextafter(u, np.float32(-1.0)))
+    return out
+
+
+def well_conditioned(oracle, inp, o32, o64):
+    """Per record and column: True where the output is held to the bound."""
+    spread = rel_err(o32, o64)
+    for seed in (1, 2, 3, 4):
+        nb = neighbour(inp, seed)
+        spread = np.maximum(spread, rel_err(oracle.bsdf(nb, 0), oracle.bsdf(nb, 1)))
+    with np.errstate(invalid="ignore"):
+        return spread <= COND
+
+
+def check_against_fp64(g, o32, inp, oracle, label):
+    """Max error of g vs the FP64 transcription over the well-conditioned finite
+    records of every column; returns {column: (max error, excluded fraction)}."""
+    o64 = oracle.bsdf(inp, 1)
+    ok = well_conditioned(oracle, inp, o32, o64)
+    err_all = rel_err(g, o64)
     report = {}
     for c in BSDF_COLS:
         fin = np.isfinite(o64[:, c]) & np.isfinite(o32[:, c])
@@ -39,10 +91,10 @@ def check_against_fp64(g, o32, o64, label):
         # an ulp of sin / cos may move a record across that edge: at most 1 in 10^4
         assert (np.isfinite(g[:, c]) != np.isfinite(o32[:, c])).mean() <= 1e-4, (label, c)
         fin &= np.isfinite(g[:, c])
-        cond = fin & (_rel(o32[:, c], o64[:, c]) <= COND)
+        cond = fin & ok[:, c]
         excluded = 1.0 - cond.sum() / max(1, fin.sum())
         assert excluded <= EXCLUDE_CAP.get(c, EXCLUDE_CAP_DEFAULT), (label, c, excluded)
-        err = float(_rel(g[cond, c], o64[cond, c]).max()) if cond.any() else 0.0
+        err = float(err_all[cond, c].max()) if cond.any() else 0.0
         report[c] = (err, excluded)
         assert err < TOL, (label, c, err, excluded)
     return report

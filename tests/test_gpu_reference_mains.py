@@ -46,9 +46,11 @@ MAINS = {
 
 
 def relmse(x, r):
+    """relMSE over the entries finite in both images."""
     x = x.astype(np.float64)
     r = r.astype(np.float64)
-    return float(np.mean((x - r) ** 2 / (r * r + 1e-2)))
+    ok = np.isfinite(x) & np.isfinite(r)
+    return float(np.mean((x[ok] - r[ok]) ** 2 / (r[ok] * r[ok] + 1e-2)))
 
 
 def _decode_png(path):
@@ -182,9 +184,15 @@ def test_reference_main_matches_oracle(gpu, oracle, programs, prog, tmp_path):
     o_rgb, _, _, _ = osc.render()
     st2 = scenes.RenderSettings(**{**st.__dict__, "seed": 101})
     noise = relmse(osc.render(settings=st2)[0], o_rgb)
-    assert np.isfinite(img).all() and img.mean() > 1e-3
+    # libWR's roughness-0 mirror (material showcase) gives D = 0/0: paths that reach
+    # it carry NaN into their pixel in the reference too; those pixels must coincide
+    bad, obad = ~np.isfinite(img).all(-1), ~np.isfinite(o_rgb).all(-1)
+    assert abs(int(bad.sum()) - int(obad.sum())) <= 1 and (bad & obad).sum() >= bad.sum() - 1
+    assert bad.mean() < 0.05 and np.nanmean(np.where(np.isfinite(img), img, np.nan)) > 1e-3
     err = relmse(img, o_rgb)
     assert err < 0.01 * noise, (prog, err, noise)
 
-    # the PNG: libWR's own writer applied to that float image
-    assert np.array_equal(_decode_png(png), oracle.tonemap(img.reshape(-1, 3)).reshape(h, w, 3))
+    # the PNG: libWR's own writer applied to that float image (finite pixels; a NaN
+    # pixel's byte is whatever the float->uint8 conversion of NaN gives)
+    want = oracle.tonemap(img.reshape(-1, 3)).reshape(h, w, 3)
+    assert np.array_equal(_decode_png(png)[~bad], want[~bad])

@@ -70,8 +70,16 @@ def _check_level2(t, p, t64, p64):
     # t of every ray whose primitive agrees (a ray that grazes a silhouette may hit
     # another surface in FP32 than in FP64: that is a primitive disagreement)
     hit = (p == p64) & (p != miss)
-    rel = np.abs(t[hit].astype(np.float64) - t64[hit]) / np.abs(t64[hit])
-    assert rel.max() < 1e-5, rel.max()
+    # t relative to 1e-5 for hits at least 1e-3 away.  Closer than that (random rays
+    # may start within 1e-5 of a surface; the renderer offsets every ray origin 1e-4)
+    # the FP32 rounding of the origin coordinates alone, ~6e-8 absolute at unit
+    # scale, exceeds 1e-5 of t: there t is held to 1e-8 absolute.
+    far = hit & (t64 >= 1e-3)
+    near = hit & (t64 < 1e-3)
+    with np.errstate(invalid="ignore"):  # inf - inf on rays that miss
+        dt = np.abs(t.astype(np.float64) - t64.astype(np.float64))
+    assert (dt[far] / t64[far]).max() < 1e-5, (dt[far] / t64[far]).max()
+    assert not near.any() or dt[near].max() < 1e-8, dt[near].max()
     return agree
 
 
