@@ -416,10 +416,15 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uin
     }
     HitAttr h = hit_program(s, r.o, r.d, h4.x, prim, mat, leafPos);
     const bool matOk = mat < s.numMats;
+    // getMaterialAlbedo is a pure function of (material, uv): fetched once for the
+    // first-hit guide and the Lambert / dielectric shading (their buckets only ever
+    // hold valid material ids)
+    constexpr bool kShadeAlbedo = kBucket == kBucketLambert || kBucket == kBucketDielectric;
+    float3 al = f3(0.0f, 0.0f, 0.0f);
+    if (kShadeAlbedo || (matOk && (r.flags & kFlagFirstHit))) al = albedo_of(s, s.mats[mat], h.u, h.v);
     // first-hit guides (trace.cu:267-286)
     if (r.flags & kFlagFirstHit) {
         if (matOk) {
-            float3 al = albedo_of(s, s.mats[mat], h.u, h.v);
             if (f.albedo) atomicAdd(f.albedo + r.pixel, make_float4(al.x, al.y, al.z, 0.0f));
             if (f.normal) atomicAdd(f.normal + r.pixel, make_float4(h.ng.x, h.ng.y, h.ng.z, 0.0f));
         }
@@ -448,8 +453,6 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uin
     const wrk_material& m = s.mats[mat];
     if (m.normalTextureId > 0) h.n = normal_mapped(s, m, h);
     if (kBucket == kBucketLambert) {
-        // getMaterialAlbedo is a pure function of (material, uv): fetch it once
-        const float3 al = albedo_of(s, m, h.u, h.v);
         bool shadow = false;
         if (f.useNEE && s.numEmissive > 0) {
             LightSample ls;
@@ -529,7 +532,6 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uin
         if (ci < 0.0f) { ci = -ci; n = neg(n); ei = m.ior; et = 1.0f; }
         float F = fresnel_dielectric(ci, ei, et);
         float xi = rnd_dim(r.seed, r.dim++);
-        float3 al = albedo_of(s, m, h.u, h.v);
         if (xi < F) {
             r.d = sub(r.d, mul(n, 2.0f * dot(r.d, n)));
             r.thr = f3(r.thr.x * al.x, r.thr.y * al.y, r.thr.z * al.z);
