@@ -156,6 +156,7 @@ struct Frame {
     float tanHalf, aspect, focal, lens;
     uint32_t width, height;
     uint32_t tilesX, perSample;  // 8x4 pixel tiles across the image (0 = row order); work items per sample
+    uint32_t interleave;         // K samples of a pixel on adjacent work items (1, 2 or 4; 1 in row order)
     uint32_t spp, useNEE, maxBounces, seed, maxIter, sampleOffset;
     float rrStart, fireflyClamp;
     uint32_t scene;  // index into Queues::scenes
