@@ -726,8 +726,8 @@ void fill_frame(Frame& f, const wrk_camera& cam, const wrk_render_params& p) {
     f.fireflyClamp = p.fireflyClamp;
     f.tilesX = (p.width % 8 == 0 && p.height % 4 == 0) ? p.width / 8 : 0;
     f.perSample = p.width * p.height;
-    // adjacent work items take K samples of one pixel, so a warp's camera paths cover
-    // 32/K pixels x K samples and their first-hit guide sums merge before the atomic
+    // adjacent work items take K samples of one pixel: a warp's camera paths cover
+    // 32/K pixels x K samples (a tighter bundle of primary rays than 32 pixels)
     f.interleave = !f.tilesX ? 1u : (p.spp % 4 == 0 ? 4u : (p.spp % 2 == 0 ? 2u : 1u));
     f.flags = p.flags;
 }

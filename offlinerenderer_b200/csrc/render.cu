@@ -394,32 +394,6 @@ struct ShadowOut {
     bool answered;      // the shadow query was answered here (the light blocks the ray)
 };
 
-// Adds a first-hit guide (trace.cu:267-286) to its pixel's sums.  Called by the lanes
-// of a warp that shade a first hit, together: lanes of one request and pixel (the
-// generator puts up to 4 samples of a pixel on adjacent work items) are summed in
-// lane order by the lowest of them, which issues one albedo and one normal atomic
-// for the group.
-__device__ __forceinline__ void add_guides(const Frame& f, uint32_t slot, uint32_t pixel, float3 al, float3 ng) {
-    __shared__ float4 sA[kShadeBlock], sN[kShadeBlock];
-    const uint32_t mask = __activemask();
-    const uint32_t peers = __match_any_sync(mask, ((unsigned long long)slot << 32) | pixel);
-    sA[threadIdx.x] = make_float4(al.x, al.y, al.z, 0.0f);
-    sN[threadIdx.x] = make_float4(ng.x, ng.y, ng.z, 0.0f);
-    __syncwarp(mask);
-    const uint32_t lane = threadIdx.x & 31u, wbase = threadIdx.x & ~31u;
-    if ((uint32_t)(__ffs(peers) - 1) == lane) {
-        float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), n = a;
-        for (uint32_t m = peers; m; m &= m - 1) {
-            const float4 x = sA[wbase + __ffs(m) - 1], y = sN[wbase + __ffs(m) - 1];
-            a = make_float4(a.x + x.x, a.y + x.y, a.z + x.z, 0.0f);
-            n = make_float4(n.x + y.x, n.y + y.y, n.z + y.z, 0.0f);
-        }
-        atomicAdd(f.albedo + pixel, a);
-        atomicAdd(f.normal + pixel, n);
-    }
-    __syncwarp(mask);
-}
-
 // Shades entry i of a bucket; the path's next state is left in r (and so for a
 // shadow ray).  Returns kOutExt / kOutShadow for a continuing path, kOutDone when
 // it ended (accumulated or dropped).
@@ -455,7 +429,10 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uin
     if (kShadeAlbedo || (matOk && (r.flags & kFlagFirstHit))) al = albedo_of(s, s.mats[mat], h.u, h.v);
     // first-hit guides (trace.cu:267-286)
     if (r.flags & kFlagFirstHit) {
-        if (matOk && f.albedo && f.normal) add_guides(f, slot_of(st.w), r.pixel, al, h.ng);
+        if (matOk) {
+            if (f.albedo) atomicAdd(f.albedo + r.pixel, make_float4(al.x, al.y, al.z, 0.0f));
+            if (f.normal) atomicAdd(f.normal + r.pixel, make_float4(h.ng.x, h.ng.y, h.ng.z, 0.0f));
+        }
         r.flags &= ~kFlagFirstHit;
     }
     int out = kOutNone;

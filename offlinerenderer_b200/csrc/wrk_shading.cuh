@@ -62,13 +62,25 @@ __device__ __forceinline__ void frame(float3 n, float3& t, float3& b) {
 __device__ __forceinline__ float3 to_world(float3 v, float3 n, float3 t, float3 b) {
     return f3(t.x * v.x + b.x * v.y + n.x * v.z, t.y * v.x + b.y * v.y + n.y * v.z, t.z * v.x + b.z * v.y + n.z * v.z);
 }
+// sin / cos / pow of the sampling and Fresnel formulas, correctly rounded: CUDA's
+// double-precision functions rounded once to float.  The sampled directions and the
+// VNDF pdf are sensitive to the last bit of these values (the GGX D term near its
+// peak multiplies an error of the half-vector by ~1/a^2), so the device rounds them
+// the one reproducible way; the oracle's matching mode does the same on the host.
+__device__ __forceinline__ void sincos_cr(float x, float& s, float& c) {
+    double sd, cd;
+    sincos((double)x, &sd, &cd);
+    s = (float)sd;
+    c = (float)cd;
+}
+__device__ __forceinline__ float pow_cr(float x, float y) { return (float)pow((double)x, (double)y); }
 __device__ __forceinline__ float3 cosine_hemisphere(float u1, float u2, float& pdf) {
     float r = sqrtf(u1);
     float th = 2.0f * kPi * u2;
     float z = sqrtf(fmaxf(0.0f, 1.0f - u1));
     pdf = z / kPi;
     float sn, cs;
-    sincosf(th, &sn, &cs);
+    sincos_cr(th, sn, cs);
     return f3(r * cs, r * sn, z);
 }
 __device__ __forceinline__ float cosine_pdf(float c) { return fmaxf(0.0f, c / kPi); }
@@ -155,7 +167,7 @@ __device__ __forceinline__ float3 ggx_eval(float3 wo, float3 wi, float3 n, float
     f0 = f0 * f0;
     float3 F0 = f3(f0 * (1.0f - metal) + alb.x * metal, f0 * (1.0f - metal) + alb.y * metal,
                    f0 * (1.0f - metal) + alb.z * metal);
-    float fw = powf(1.0f - voh, 5.0f);
+    float fw = pow_cr(1.0f - voh, 5.0f);
     float3 F = f3(F0.x + (1.0f - F0.x) * fw, F0.y + (1.0f - F0.y) * fw, F0.z + (1.0f - F0.z) * fw);
     float den = 4.0f * nov * nol;
     float3 spec = f3(D * G * F.x / den, D * G * F.y / den, D * G * F.z / den);
@@ -193,7 +205,7 @@ __device__ __forceinline__ void ggx_sample(float3 wo, float3 n, float3 tg, float
     bool lower = u1 < ia;
     float phi = kPi * (lower ? u1 / ia : 1.0f + (u1 - ia) / (1.0f - ia));
     float sp, cp;
-    sincosf(phi, &sp, &cp);
+    sincos_cr(phi, sp, cp);
     float p1 = r * cp;
     float p2 = r * sp * (lower ? 1.0f : sv.z);
     float sq = sqrtf(fmaxf(0.0f, 1.0f - (p1 * p1 + p2 * p2)));

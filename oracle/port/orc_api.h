@@ -86,7 +86,8 @@ void orc_camera_rays(const orc_camera* cam, uint32_t width, uint32_t height, con
                      const uint32_t* samples, uint32_t n, uint32_t seed, float* out);
 
 // Per-function batches (FP32 when prec == 0, FP64 transcription when prec == 1,
-// results returned as double).  See orc_api.cpp for the record layouts.
+// FP32 with correctly rounded sin / cos / pow -- the device library's -- when prec
+// == 2; results returned as double).  See orc_api.cpp for the record layouts.
 void orc_bsdf_batch(const float* in, uint32_t n, int prec, double* out);
 void orc_rng_batch(const uint32_t* seeds, const uint32_t* dims, uint32_t n, uint32_t* hash, float* u);
 void orc_cdf_batch(const float* cdf, uint32_t ncdf, const float* u, uint32_t n, uint32_t* out);

@@ -594,10 +594,12 @@ void orc_camera_rays(const orc_camera* cam, uint32_t w, uint32_t h, const uint32
 //  20-22 frame tangent(n)  23-25 bitangent  26-28 sample_triangle(u0,u1; wo,wi,n)
 //  29 its area  30-32 its normal  33 shading_correction(wi, n, normalize(wo))
 void orc_bsdf_batch(const float* in, uint32_t n, int prec, double* out) {
+    cr_elementary() = prec == 2;
     for (uint32_t i = 0; i < n; ++i) {
-        if (prec == 0) bsdf_one<float>(in + 20 * (size_t)i, out + 34 * (size_t)i);
+        if (prec == 0 || prec == 2) bsdf_one<float>(in + 20 * (size_t)i, out + 34 * (size_t)i);
         else bsdf_one<double>(in + 20 * (size_t)i, out + 34 * (size_t)i);
     }
+    cr_elementary() = 0;
 }
 
 void orc_rng_batch(const uint32_t* seeds, const uint32_t* dims, uint32_t n, uint32_t* hash, float* u) {

@@ -20,6 +20,25 @@ namespace orc {
 // kPi = 3.14159265f (materials/material_common.cuh:9); both round to the same float.
 template <class T> constexpr T kPiT() { return T(3.14159265358979323846f); }
 
+// Elementary functions of the FP32 restatement.  By default glibc's sinf / cosf /
+// powf, as the reference's shading headers get them when built on the host (the
+// bit-exact pin against that build).  With cr_elementary() set, the correctly
+// rounded value -- computed in double and rounded once to float -- which is what
+// the device library evaluates; the GPU parity tests use that mode so the device
+// and the restatement round alike.  The double instantiation is unaffected.
+inline int& cr_elementary() {
+    static thread_local int mode = 0;
+    return mode;
+}
+template <class T> inline T esin(T x) { return std::sin(x); }
+template <class T> inline T ecos(T x) { return std::cos(x); }
+template <class T> inline T epow(T x, T y) { return std::pow(x, y); }
+template <> inline float esin<float>(float x) { return cr_elementary() ? (float)std::sin((double)x) : std::sin(x); }
+template <> inline float ecos<float>(float x) { return cr_elementary() ? (float)std::cos((double)x) : std::cos(x); }
+template <> inline float epow<float>(float x, float y) {
+    return cr_elementary() ? (float)std::pow((double)x, (double)y) : std::pow(x, y);
+}
+
 template <class T> struct V3 {
     T x, y, z;
 };
@@ -87,7 +106,7 @@ template <class T> inline V3<T> cosine_hemisphere(T u1, T u2, T& pdf) {
     T th = T(2) * kPiT<T>() * u2;
     T z = std::sqrt(std::fmax(T(0), T(1) - u1));
     pdf = z / kPiT<T>();
-    return {r * std::cos(th), r * std::sin(th), z};
+    return {r * ecos(th), r * esin(th), z};
 }
 template <class T> inline T cosine_pdf(T c) { return std::fmax(T(0), c / kPiT<T>()); }
 template <class T>
@@ -163,7 +182,7 @@ template <class T> inline T ggx_G1(T nov, T a) {
     return T(2) * nov / (nov + std::sqrt(a2 + (T(1) - a2) * c2));
 }
 template <class T> inline V3<T> schlick3(T voh, V3<T> f0) {
-    T f = std::pow(T(1) - voh, T(5));
+    T f = epow(T(1) - voh, T(5));
     return {f0.x + (T(1) - f0.x) * f, f0.y + (T(1) - f0.y) * f, f0.z + (T(1) - f0.z) * f};
 }
 template <class T> inline V3<T> mix_f0(V3<T> alb, T metal, T ior) {
@@ -220,7 +239,7 @@ inline bool ggx_sample(V3<T> wo, V3<T> n, V3<T> tg, V3<T> bt, T rough, T u0, T u
     T r = std::sqrt(u0);
     bool lower = u1 < ia;
     T phi = kPiT<T>() * (lower ? u1 / ia : T(1) + (u1 - ia) / (T(1) - ia));
-    T sp = std::sin(phi), cp = std::cos(phi);
+    T sp = esin(phi), cp = ecos(phi);
     T p1 = r * cp;
     T p2 = r * sp * (lower ? T(1) : sv.z);
     T sq = std::sqrt(std::fmax(T(0), T(1) - (p1 * p1 + p2 * p2)));

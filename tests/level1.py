@@ -9,18 +9,17 @@ normal -- are compared relative to the vector's length: a unit direction's
 component near zero has no meaningful relative precision of its own.
 
 Condition criterion.  A record is left out of an output's bound only where that
-output is ill-conditioned in FP32 there: where the reference's OWN FP32
-arithmetic (the oracle's FP32 port, bit-identical to the reference build
-compiled on the host) differs from FP64 by more than half the tolerance, at the
-record or at any of four neighbouring records whose random numbers u0..u2 are
-one float32 ulp away.  The neighbours matter because FP32 rounding error near an
-ill-conditioned point is erratic -- one evaluation may land close to FP64 by
-chance -- and because a one-ulp change of a random number moves the sampling
-angle by as much as the one- or two-ulp differences between CUDA's and glibc's
-sin / cos.  Example: the GGX D term near its peak at low roughness, where
-1 - NoH^2 (1 - a^2) cancels and multiplies the rounding of NoH by about 1/a^2.
-The excluded fraction is capped per column (measured on the seeded inputs;
-roughness U(0.05, 1)).
+output is ill-conditioned in FP32 there: where the FP32 evaluation of the
+reference's formulas (the oracle's FP32 port, operation for operation the
+reference's order; for the device comparison in its mode with correctly rounded
+sin / cos / pow, the rounding the device library uses) differs from FP64 by more
+than half the tolerance, at the record or at any of four neighbouring records
+whose random numbers u0..u2 are one float32 ulp away.  The neighbours matter
+because FP32 rounding error near an ill-conditioned point is erratic: one
+evaluation may land close to FP64 by chance.  Example: the GGX D term near its
+peak at low roughness, where 1 - NoH^2 (1 - a^2) cancels and multiplies the
+rounding of NoH by about 1/a^2.  The excluded fraction is capped per column
+(measured on the seeded inputs; roughness U(0.05, 1)).
 """
 import numpy as np
 
@@ -68,21 +67,23 @@ def neighbour(inp, seed):
     return out
 
 
-def well_conditioned(oracle, inp, o32, o64):
-    """Per record and column: True where the output is held to the bound."""
+def well_conditioned(oracle, inp, o32, o64, prec=0):
+    """Per record and column: True where the output is held to the bound.  o32 is
+    the oracle's FP32 evaluation in mode `prec` (0: glibc's elementary functions,
+    as the reference's host build; 2: correctly rounded ones, as the device)."""
     spread = rel_err(o32, o64)
     for seed in (1, 2, 3, 4):
         nb = neighbour(inp, seed)
-        spread = np.maximum(spread, rel_err(oracle.bsdf(nb, 0), oracle.bsdf(nb, 1)))
+        spread = np.maximum(spread, rel_err(oracle.bsdf(nb, prec), oracle.bsdf(nb, 1)))
     with np.errstate(invalid="ignore"):
         return spread <= COND
 
 
-def check_against_fp64(g, o32, inp, oracle, label):
+def check_against_fp64(g, o32, inp, oracle, label, prec=0):
     """Max error of g vs the FP64 transcription over the well-conditioned finite
     records of every column; returns {column: (max error, excluded fraction)}."""
     o64 = oracle.bsdf(inp, 1)
-    ok = well_conditioned(oracle, inp, o32, o64)
+    ok = well_conditioned(oracle, inp, o32, o64, prec)
     err_all = rel_err(g, o64)
     report = {}
     for c in BSDF_COLS:
