@@ -189,7 +189,12 @@ def served_legs(args, rend, local):
                                                    "peak": peak, "unit": "TFLOP/s",
                                                    "frac": flops / (ms / 1e3) / 1e12 / peak, "peak_source": kind,
                                                    "flop_per_launch": flops},
-                       "weights": {k: meta[k] for k in ("scenes", "target_spp", "steps", "final_loss") if k in meta}}
+                       "weights": dict({k: meta[k] for k in ("views", "size", "target_spp", "input_spps", "steps",
+                                                             "final_loss") if k in meta},
+                                       scene_seeds=f"{min(meta['scenes'])}-{max(meta['scenes'])}" if "scenes" in meta
+                                       else None,
+                                       pairs=len(meta.get("scenes", [])) * meta.get("views", 0)
+                                       * len(meta.get("input_spps", [])))}}
     # time to the plain 256-spp relMSE against an FP64-accumulated reference
     rs = {}
     ref = quality.reference(rend, scene, cam, st, total_spp=args.ref_spp, chunk=256, stats=rs)
