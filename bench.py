@@ -146,6 +146,15 @@ def bf16_peak():
         return FALLBACK_BF16_TFLOPS, "fallback"
 
 
+def weights_summary(meta: dict) -> dict:
+    """What the committed denoiser weights were trained on (their metadata)."""
+    out = {k: meta[k] for k in ("views", "size", "target_spp", "input_spps", "steps", "final_loss") if k in meta}
+    if "scenes" in meta:
+        out["scene_seeds"] = f"{min(meta['scenes'])}-{max(meta['scenes'])}"
+        out["pairs"] = len(meta["scenes"]) * meta.get("views", 0) * len(meta.get("input_spps", []))
+    return out
+
+
 def served_legs(args, rend, local):
     """Denoiser throughput, time-to-relMSE and the serving workload on the scale
     scene (1920x1080, ~2.41M triangles), with the committed denoiser weights."""
@@ -189,12 +198,7 @@ def served_legs(args, rend, local):
                                                    "peak": peak, "unit": "TFLOP/s",
                                                    "frac": flops / (ms / 1e3) / 1e12 / peak, "peak_source": kind,
                                                    "flop_per_launch": flops},
-                       "weights": dict({k: meta[k] for k in ("views", "size", "target_spp", "input_spps", "steps",
-                                                             "final_loss") if k in meta},
-                                       scene_seeds=f"{min(meta['scenes'])}-{max(meta['scenes'])}" if "scenes" in meta
-                                       else None,
-                                       pairs=len(meta.get("scenes", [])) * meta.get("views", 0)
-                                       * len(meta.get("input_spps", [])))}}
+                       "weights": weights_summary(meta)}
     # time to the plain 256-spp relMSE against an FP64-accumulated reference
     rs = {}
     ref = quality.reference(rend, scene, cam, st, total_spp=args.ref_spp, chunk=256, stats=rs)
