@@ -25,6 +25,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "wrk_internal.h"
@@ -719,6 +720,40 @@ __global__ void k_sah(const uint4* __restrict__ nodes, uint32_t numNodes, double
 
 }  // namespace
 
+// The build's scratch (primitive references, tasks, bins, the binary tree, ...: a few
+// hundred MB for a 2.4M-triangle scene) comes from a stream-ordered memory pool of
+// the library's own, one per device, that keeps its memory between builds: no
+// cudaMalloc / cudaFree in the build, and a scene built after another reuses the
+// same memory.  The finished tree (nodes, triangle records) is allocated with
+// cudaMalloc, as it lives with the scene.
+cudaError_t scratch_pool(cudaMemPool_t* out) {
+    static std::mutex m;
+    static cudaMemPool_t pools[64] = {nullptr};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(m);
+    if (!pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if ((e = cudaMemPoolCreate(&p, &props)) != cudaSuccess) return e;
+        unsigned long long keep = ~0ull;  // never hand memory back at synchronisation
+        if ((e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+        pools[dev] = p;
+    }
+    *out = pools[dev];
+    return cudaSuccess;
+}
+
+template <class T>
+cudaError_t scratch_alloc(T** p, cudaMemPool_t pool, cudaStream_t st, size_t bytes) {
+    return cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, pool, st);
+}
+
 #define WRK_BCHECK(x)                                                                               \
     do {                                                                                            \
         cudaError_t e_ = (x);                                                                       \
@@ -756,32 +791,34 @@ int build_bvh8(const float* d_vtx, const uint32_t* d_idx, const uint32_t* d_triM
     int rc = WRK_ERR_CUDA;
     std::vector<uint32_t> iota;
 
+    cudaMemPool_t pool = nullptr;
+    WRK_BCHECK(scratch_pool(&pool));
     WRK_BCHECK(cudaEventCreate(&e0));
     WRK_BCHECK(cudaEventCreate(&e1));
     WRK_BCHECK(cudaEventRecord(e0, st));
-    WRK_BCHECK(cudaMalloc(&blo, sizeof(float4) * n));
-    WRK_BCHECK(cudaMalloc(&bhi, sizeof(float4) * n));
-    WRK_BCHECK(cudaMalloc(&ref, sizeof(uint32_t) * n));
-    WRK_BCHECK(cudaMalloc(&ref2, sizeof(uint32_t) * n));
-    WRK_BCHECK(cudaMalloc(&flags, sizeof(uint32_t) * n));
-    WRK_BCHECK(cudaMalloc(&scan, sizeof(uint32_t) * std::max<uint32_t>(n, 4u)));  // also the SAH sums (2 doubles)
-    WRK_BCHECK(cudaMalloc(&taskOf, sizeof(int) * n));
-    WRK_BCHECK(cudaMalloc(&taskOf2, sizeof(int) * n));
-    WRK_BCHECK(cudaMalloc(&tasks, sizeof(Task) * maxTasks));
-    WRK_BCHECK(cudaMalloc(&ntasks, sizeof(Task) * maxTasks));
-    WRK_BCHECK(cudaMalloc(&tcen, sizeof(OBox) * maxTasks));
-    WRK_BCHECK(cudaMalloc(&ncen, sizeof(OBox) * maxTasks));
-    WRK_BCHECK(cudaMalloc(&bins, sizeof(Bin) * 3 * kBins * (size_t)maxTasks));
-    WRK_BCHECK(cudaMalloc(&splits, sizeof(Split) * maxTasks));
-    WRK_BCHECK(cudaMalloc(&small, sizeof(SmallTask) * (size_t)(n + 1)));
-    WRK_BCHECK(cudaMalloc(&nodes, sizeof(BNode) * maxNodes));
-    WRK_BCHECK(cudaMalloc(&nbox, sizeof(OBox) * maxNodes));
-    WRK_BCHECK(cudaMalloc(&fromLevels, maxNodes));
-    WRK_BCHECK(cudaMalloc(&ctr, sizeof(BuildCtr)));
+    WRK_BCHECK(scratch_alloc(&blo, pool, st, sizeof(float4) * n));
+    WRK_BCHECK(scratch_alloc(&bhi, pool, st, sizeof(float4) * n));
+    WRK_BCHECK(scratch_alloc(&ref, pool, st, sizeof(uint32_t) * n));
+    WRK_BCHECK(scratch_alloc(&ref2, pool, st, sizeof(uint32_t) * n));
+    WRK_BCHECK(scratch_alloc(&flags, pool, st, sizeof(uint32_t) * n));
+    WRK_BCHECK(scratch_alloc(&scan, pool, st, sizeof(uint32_t) * std::max<uint32_t>(n, 4u)));  // also the SAH sums (2 doubles)
+    WRK_BCHECK(scratch_alloc(&taskOf, pool, st, sizeof(int) * n));
+    WRK_BCHECK(scratch_alloc(&taskOf2, pool, st, sizeof(int) * n));
+    WRK_BCHECK(scratch_alloc(&tasks, pool, st, sizeof(Task) * maxTasks));
+    WRK_BCHECK(scratch_alloc(&ntasks, pool, st, sizeof(Task) * maxTasks));
+    WRK_BCHECK(scratch_alloc(&tcen, pool, st, sizeof(OBox) * maxTasks));
+    WRK_BCHECK(scratch_alloc(&ncen, pool, st, sizeof(OBox) * maxTasks));
+    WRK_BCHECK(scratch_alloc(&bins, pool, st, sizeof(Bin) * 3 * kBins * (size_t)maxTasks));
+    WRK_BCHECK(scratch_alloc(&splits, pool, st, sizeof(Split) * maxTasks));
+    WRK_BCHECK(scratch_alloc(&small, pool, st, sizeof(SmallTask) * (size_t)(n + 1)));
+    WRK_BCHECK(scratch_alloc(&nodes, pool, st, sizeof(BNode) * maxNodes));
+    WRK_BCHECK(scratch_alloc(&nbox, pool, st, sizeof(OBox) * maxNodes));
+    WRK_BCHECK(scratch_alloc(&fromLevels, pool, st, maxNodes));
+    WRK_BCHECK(scratch_alloc(&ctr, pool, st, sizeof(BuildCtr)));
     WRK_BCHECK(cudaMemsetAsync(fromLevels, 0, maxNodes, st));
     WRK_BCHECK(cudaMemsetAsync(ctr, 0, sizeof(BuildCtr), st));
     WRK_BCHECK(cub::DeviceScan::ExclusiveSum(nullptr, cubBytes, flags, scan, (int)n, st));
-    WRK_BCHECK(cudaMalloc(&cubTmp, cubBytes));
+    WRK_BCHECK(scratch_alloc(&cubTmp, pool, st, cubBytes));
 
     iota.resize(n);
     for (uint32_t i = 0; i < n; ++i) iota[i] = i;
@@ -852,9 +889,9 @@ int build_bvh8(const float* d_vtx, const uint32_t* d_idx, const uint32_t* d_triM
     numBinary = hc.nodes;
 
     // ---- collapse ----
-    WRK_BCHECK(cudaMalloc(&items, sizeof(CItem) * numBinary));
-    WRK_BCHECK(cudaMalloc(&items2, sizeof(CItem) * numBinary));
-    WRK_BCHECK(cudaMalloc(&cctr, sizeof(CollapseCtr)));
+    WRK_BCHECK(scratch_alloc(&items, pool, st, sizeof(CItem) * numBinary));
+    WRK_BCHECK(scratch_alloc(&items2, pool, st, sizeof(CItem) * numBinary));
+    WRK_BCHECK(scratch_alloc(&cctr, pool, st, sizeof(CollapseCtr)));
     WRK_BCHECK(cudaMalloc(&onodes, sizeof(uint4) * 5 * (size_t)numBinary));
     WRK_BCHECK(cudaMalloc(&otris, sizeof(float4) * 3 * (size_t)n));
     {
@@ -915,10 +952,12 @@ int build_bvh8(const float* d_vtx, const uint32_t* d_idx, const uint32_t* d_triM
         rc = WRK_OK;
     }
 fail:
-    cudaFree(blo); cudaFree(bhi); cudaFree(ref); cudaFree(ref2); cudaFree(flags); cudaFree(scan);
-    cudaFree(taskOf); cudaFree(taskOf2); cudaFree(tasks); cudaFree(ntasks); cudaFree(tcen); cudaFree(ncen);
-    cudaFree(bins); cudaFree(splits); cudaFree(small); cudaFree(nodes); cudaFree(nbox); cudaFree(fromLevels);
-    cudaFree(ctr); cudaFree(cubTmp); cudaFree(items); cudaFree(items2); cudaFree(cctr); cudaFree(onodes);
+    for (void* p : {(void*)blo, (void*)bhi, (void*)ref, (void*)ref2, (void*)flags, (void*)scan, (void*)taskOf,
+                    (void*)taskOf2, (void*)tasks, (void*)ntasks, (void*)tcen, (void*)ncen, (void*)bins, (void*)splits,
+                    (void*)small, (void*)nodes, (void*)nbox, (void*)fromLevels, (void*)ctr, cubTmp, (void*)items,
+                    (void*)items2, (void*)cctr})
+        if (p) cudaFreeAsync(p, st);
+    cudaFree(onodes);
     cudaFree(otris);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
