@@ -397,12 +397,15 @@ def main():
     rend.set_launch(tune["chunk"], tune["shadeBlock"])
     npx = st.width * st.height
     frame = torch.zeros(npx * 3, dtype=torch.float32, device=f"cuda:{local}")
+    # the workload's output: radiance plus the first-hit albedo and normal guides
+    guides = torch.zeros(2, npx * 3, dtype=torch.float32, device=f"cuda:{local}")
     samples_per_step = npx * st.spp
 
     def step(i):
         off = (i * world + rank) * st.spp
         # TensorPtr waits for torch's stream (the previous step's all-reduce reads the frame)
-        s = rend.render_device(scene, None, d_rgb_ptr=wrk.TensorPtr(frame).ptr, sample_offset=off)
+        s = rend.render_device(scene, None, d_rgb_ptr=wrk.TensorPtr(frame).ptr, sample_offset=off,
+                               d_albedo=wrk.TensorPtr(guides[0]), d_normal=wrk.TensorPtr(guides[1]))
         if dist is not None:
             dist.all_reduce(frame)  # combine the ranks' sample ranges
         return s
@@ -440,7 +443,8 @@ def main():
     mqueries = world * queries / (ms / 1e3) / 1e6
 
     # per-stage device times (events on the renderer's stream), one extra render
-    tst = rend.render_device(scene, None, d_rgb_ptr=wrk.TensorPtr(frame).ptr, stage_timing=True)
+    tst = rend.render_device(scene, None, d_rgb_ptr=wrk.TensorPtr(frame).ptr, stage_timing=True,
+                             d_albedo=wrk.TensorPtr(guides[0]), d_normal=wrk.TensorPtr(guides[1]))
     stage_ms = tst["stageMs"]
     units = {"trace_extension": tst["extensionRays"], "trace_shadow": tst["shadowTraced"],
              "shade_lambert": tst["bucketPaths"]["lambert"], "shade_dielectric": tst["bucketPaths"]["dielectric"],

@@ -744,8 +744,10 @@ static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, con
     int rc = r->frameBufs.alloc(np * 3 * sizeof(float4));
     if (rc) return rc;
     f.accum = r->frameBufs.as<float4>();
-    f.albedo = f.accum + np;
-    f.normal = f.albedo + np;
+    // first-hit guides are summed only when the caller asks for them (two atomics
+    // per camera path, ~4 % of a showcase render)
+    f.albedo = d_alb ? f.accum + np : nullptr;
+    f.normal = d_nrm ? f.accum + 2 * np : nullptr;
     f.err = &E.q.ctr->error;
     f.scene = 0;
     cudaStream_t st = E.stream;

@@ -426,7 +426,7 @@ __device__ __forceinline__ int shade_one(const DevScene& s, const PathQ& in, uin
     // hold valid material ids)
     constexpr bool kShadeAlbedo = kBucket == kBucketLambert || kBucket == kBucketDielectric;
     float3 al = f3(0.0f, 0.0f, 0.0f);
-    if (kShadeAlbedo || (matOk && (r.flags & kFlagFirstHit))) al = albedo_of(s, s.mats[mat], h.u, h.v);
+    if (kShadeAlbedo || (matOk && f.albedo && (r.flags & kFlagFirstHit))) al = albedo_of(s, s.mats[mat], h.u, h.v);
     // first-hit guides (trace.cu:267-286)
     if (r.flags & kFlagFirstHit) {
         if (matOk) {
