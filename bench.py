@@ -67,9 +67,9 @@ UNET_FLOP_PER_PX = sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in UNET_LAYERS)
 # Measured DRAM traffic of the extension-ray traversal kernel per ray: ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) summed over the 12 launches of the
 # 512x512 16-spp render of the same scene that ncu profiles (the plain-launch,
-# stage-timed one), divided by its 14,406,476 extension rays; traffic per launch of
+# stage-timed one), divided by its 14,406,486 extension rays; traffic per launch of
 # the full workload = this x rays per launch (traffic grows with the rays traced).
-TRACE_EXT_TRAFFIC_BYTES_PER_RAY = 148.5
+TRACE_EXT_TRAFFIC_BYTES_PER_RAY = 149.2
 # SM issue-slot utilisation of the traversal and shading kernels (the roofline that
 # bounds them: SIMT integer / FP32 work, not HBM), smsp__issue_active from ncu --set
 # full on the 16-spp capture of the same scene.  CUDA events cannot measure it live.
