@@ -140,6 +140,28 @@ def test_convergence_to_high_spp(gpu):
     assert e[0] / e[2] > 6.0
 
 
+def test_gpu_and_oracle_converge_to_one_fp64_reference(gpu, oracle):
+    """North-star level 3, second half: the GPU renderer and the oracle converge to
+    the same FP64-accumulated 4096-spp image.  The reference is the GPU's (f32 sums
+    per 512-spp chunk accumulated in float64, sample indices from 2^20 on, disjoint
+    from the others); the oracle's own 4096-spp render is as close to it as a second
+    independent GPU 4096-spp render is (the estimator's noise floor), and the
+    oracle's error falls with spp like the GPU's."""
+    from offlinerenderer_b200 import quality
+
+    sd = scenes.cornell(32, 32, 4096, seed=1)
+    s = gpu.Scene.from_data(sd)
+    r = gpu.Renderer()
+    ref = quality.reference(r, s, sd.camera, sd.settings, total_spp=4096, chunk=512).cpu().numpy()
+    floor = relmse(r.render(s, sample_offset=8192).rgb, ref)  # an independent GPU 4096-spp estimate
+    osc = oracle.scene(sd)
+    o4096 = osc.render()[0]
+    o256 = osc.render(spp=256)[0]
+    e4096, e256 = relmse(o4096, ref), relmse(o256, ref)
+    assert e4096 < 1.5 * floor, (e4096, floor)
+    assert e256 > 6.0 * e4096, (e256, e4096)
+
+
 def test_errors_are_reported(gpu):
     sd = scenes.cornell(8, 8, 1)
     s = gpu.Scene.from_data(sd)
