@@ -161,7 +161,9 @@ int wrk_scene_light_cdf(wrk_scene* s, uint32_t* tris, float* cdf, uint32_t capac
 
 /* Copies the 8-wide BVH to host memory for inspection: nodes = numNodes * 20 u32
  * (five 16-byte words each), tris = numTriangles * 12 floats (v0|prim, e1|material,
- * e2|0 per triangle, in leaf order).  Sizes come from wrk_scene_bvh_info. */
+ * e2|bucket per triangle, in leaf order; bucket = the material's shade queue: 0
+ * Lambert, 1 glass / rough glass, 2 GGX, 3 emissive or other, as a u32).  Sizes come
+ * from wrk_scene_bvh_info. */
 int wrk_scene_bvh_export(wrk_scene* s, uint32_t* nodes, float* tris);
 
 /* Device addresses of a finalized scene's buffers: the getters of wr::Scene

@@ -261,9 +261,9 @@ static void launch_iteration(const Engine& E, const DevScene& s0, bool multi, cu
     if (ev) cudaEventRecord(ev[1], st);
     launch_generate(E.q, E.numSMs * 8, st);
     if (ev) cudaEventRecord(ev[2], st);
-    launch_trace_extension(s0, E.q, multi, E.trace_grid(), st);
+    launch_trace_extension(s0, E.q, multi, E.numSMs, st);
     if (ev) cudaEventRecord(ev[3], st);
-    launch_trace_shadow(s0, E.q, multi, E.trace_grid(), st);
+    launch_trace_shadow(s0, E.q, multi, E.numSMs, st);
     if (ev) cudaEventRecord(ev[4], st);
     // four shade kernels; the fifth stage slot (Lambert resume) stays empty: the
     // shadow kernel continues those paths
@@ -286,7 +286,6 @@ cudaError_t Engine::enqueue_chunk(const DevScene& s0, bool multi, bool timing) {
     } else {
         const bool same = graph && multi == graphMulti && memcmp(&s0, &graphScene, sizeof(DevScene)) == 0 &&
                           graphCfg.chunk == cfg.chunk && graphCfg.shadeBlock == cfg.shadeBlock &&
-                          graphCfg.traceBlocksPerSM == cfg.traceBlocksPerSM &&
                           graphCfg.shadeBlocksPerSM == cfg.shadeBlocksPerSM;
         if (!same) {
             if (graph) cudaGraphExecDestroy(graph);
@@ -314,7 +313,6 @@ cudaError_t Engine::enqueue_until_done(const DevScene& s0, bool multi, uint32_t 
     cudaError_t e;
     const bool same = loopGraph && multi == loopMulti && memcmp(&s0, &loopScene, sizeof(DevScene)) == 0 &&
                       loopCfg.chunk == cfg.chunk && loopCfg.shadeBlock == cfg.shadeBlock &&
-                      loopCfg.traceBlocksPerSM == cfg.traceBlocksPerSM &&
                       loopCfg.shadeBlocksPerSM == cfg.shadeBlocksPerSM;
     if (!same) {
         if (loopGraph) cudaGraphExecDestroy(loopGraph);
@@ -580,6 +578,11 @@ int wrk_scene_finalize(wrk_scene* s) {
     if (rc) return fail(rc, "%s", err);
     s->nodes = br.nodes;
     s->tris = br.tris;
+    // the shade bucket of each record's material, so the trace kernel sorts a hit
+    // with one load from the record it just tested
+    launch_leaf_buckets(br.tris, nt, s->dMats.as<wrk_material>(), (uint32_t)s->mats.size(), 0);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(0));
     s->info.numTriangles = nt;
     s->info.numNodes = br.numNodes;
     s->info.numBinaryNodes = br.numBinary;

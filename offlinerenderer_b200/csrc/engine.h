@@ -35,7 +35,6 @@ struct EngineBuf {
 struct LaunchConfig {
     uint32_t chunk = 8;         // iterations per graph launch / host check
     uint32_t shadeBlock = 256;  // 128 or 256 threads per shade block
-    uint32_t traceBlocksPerSM = 8;
     uint32_t shadeBlocksPerSM = 4;  // in units of 256-thread blocks
 };
 
@@ -87,7 +86,6 @@ struct Engine {
     cudaError_t enqueue_until_done(const DevScene& s0, bool multi, uint32_t iterLimit);
     // Adds the per-stage times of the last timed chunk.
     cudaError_t stage_times(float* ms, uint32_t* launches);
-    int trace_grid() const { return numSMs * (int)cfg.traceBlocksPerSM; }
     int shade_grid() const { return numSMs * (int)cfg.shadeBlocksPerSM; }
 };
 

@@ -1,7 +1,9 @@
 // Stand-alone device kernels behind the kernel-level C entry points: stable
 // ballot/prefix-sum compaction, light-CDF selection, RNG, the BSDF math batch,
 // texture fetch, camera rays, and the ACES tonemap.  These are the same device
-// functions the renderer uses, exposed one at a time for parity checks.
+// functions the renderer uses, exposed one at a time for parity checks.  Also the
+// finalize-time pass that completes the BVH's triangle records for shading.
+#include <algorithm>
 #include <mutex>
 
 #include "wrk_internal.h"
@@ -203,6 +205,21 @@ __global__ void k_tonemap(const float* __restrict__ rgb, uint32_t nfloat, uint8_
         reinterpret_cast<uchar4*>(out)[i] = b;
     }
     for (uint32_t i = n4 * 4 + blockIdx.x * blockDim.x + threadIdx.x; i < nfloat; i += stride) out[i] = aces_byte(rgb[i]);
+}
+
+__global__ void k_leaf_buckets(float4* tris, uint32_t nt, const wrk_material* __restrict__ mats, uint32_t numMats) {
+    for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nt; l += gridDim.x * blockDim.x) {
+        const uint32_t mat = __float_as_uint(tris[3 * (size_t)l + 1].w);
+        const uint32_t b = mat < numMats ? bucket_of_type(mats[mat].type) : (uint32_t)kBucketOther;
+        tris[3 * (size_t)l + 2].w = __uint_as_float(b);
+    }
+}
+
+void launch_leaf_buckets(float4* tris, uint32_t numTris, const wrk_material* mats, uint32_t numMats,
+                         cudaStream_t st) {
+    if (!numTris) return;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(((uint64_t)numTris + 255) / 256, 148u * 16u);
+    k_leaf_buckets<<<grid, 256, 0, st>>>(tris, numTris, mats, numMats);
 }
 
 void launch_cdf(const float* cdf, uint32_t ncdf, const float* u, uint32_t n, uint32_t* out, cudaStream_t st) {

@@ -646,7 +646,9 @@ __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k
         // extension buffer it will be traced from two iterations on (this
         // iteration's input, no longer read); the control kernel of the next
         // iteration starts that queue after these entries.
-        const bool cx = (ps != kInvalidSlot && so.cont == kContExt) || out == kOutCont;
+        // (decided from the outcome alone, so the three appends' atomics are issued
+        // together; a queue overflow fails the whole render, whatever is written)
+        const bool cx = (out == kOutShadow && so.cont == kContExt) || out == kOutCont;
         const uint32_t pc = append_pos(&c->cont.v, cx, q.capacity, &c->error);
         // shadow queries answered here: counted as traced, and the continuations
         // they leave (no shadow entry) held as live paths until traced

@@ -22,8 +22,11 @@
 namespace wrk {
 
 constexpr int kTraceBlock = 128;
-constexpr int kStackSmem = 12;
-constexpr int kStackLocal = 36;
+#ifndef WRK_STACK_SMEM
+#define WRK_STACK_SMEM 12
+#endif
+constexpr int kStackSmem = WRK_STACK_SMEM;
+constexpr int kStackLocal = 48 - kStackSmem;
 constexpr uint32_t kMaxVisits = 1u << 16;
 
 // Byte k of w as the float 2^15 + b, exactly, without an int->float conversion:
@@ -120,13 +123,24 @@ struct Trav {
     Ray r;
     float ix, iy, iz;
     uint32_t octInv;
-    uint32_t gBase, gHits, gImask, tBase, tMask;
+    uint32_t gBase;
+    uint32_t gBits;  // node group: child hit bits (bits 0-7, octant order) | internal-child mask << 8
+    uint32_t tBase, tMask;
     int sp;
     uint32_t visits;
     float tBest;
-    uint32_t pBest, mBest;
-    uint32_t lBest;  // leaf position (index into the BVH triangle records) of the best hit
+    // Leaf position (index into the BVH triangle records) of the best hit, kNoHit
+    // while there is none; the hit's primitive and material are read from that
+    // record when the ray is done, so they take no registers during traversal.
+    uint32_t lBest;
 };
+
+__device__ __forceinline__ uint32_t record_prim(const float4* tris, uint32_t l) {
+    return l == kNoHit ? kNoHit : __float_as_uint(__ldg(tris + 3 * (size_t)l).w);
+}
+__device__ __forceinline__ uint32_t record_material(const float4* tris, uint32_t l) {
+    return l == kNoHit ? 0u : __float_as_uint(__ldg(tris + 3 * (size_t)l + 1).w);
+}
 
 __device__ __forceinline__ void trav_init(Trav& t, const Ray& r) {
     t.r = r;
@@ -141,16 +155,13 @@ __device__ __forceinline__ void trav_init(Trav& t, const Ray& r) {
     t.octInv = oct ^ 7u;  // slot of the child nearest the entry corner -> bit 0
     // the root is a one-child node group
     t.gBase = 0;
-    t.gHits = 1u << t.octInv;
-    t.gImask = 1u;
+    t.gBits = (1u << t.octInv) | (1u << 8);
     t.tBase = 0;
     t.tMask = 0;
     t.sp = 0;
     t.visits = 0;
     t.tBest = r.tmax;
-    t.pBest = kNoHit;
-    t.mBest = 0;
-    t.lBest = 0;
+    t.lBest = kNoHit;
 }
 
 // One traversal step: descend into the next child of the current node group
@@ -165,13 +176,13 @@ __device__ __forceinline__ bool trav_step(const Geom& s, Trav& t, uint2* sstack,
         atomicOr(errFlag, kErrBadIndex);
         return true;
     }
-    if (t.gHits) {
-        uint32_t pos = __ffs(t.gHits) - 1;
-        t.gHits &= t.gHits - 1;
+    if (t.gBits & 0xffu) {
+        uint32_t pos = __ffs(t.gBits) - 1;  // the lowest set bit is a hit bit
+        t.gBits &= t.gBits - 1;
         uint32_t slot = pos ^ t.octInv;
-        uint32_t child = t.gBase + __popc(t.gImask & ((1u << slot) - 1u));
-        if (t.gHits) {
-            uint2 e = make_uint2(t.gBase, t.gHits | (t.gImask << 8));
+        uint32_t child = t.gBase + __popc(t.gBits & (((1u << slot) - 1u) << 8));
+        if (t.gBits & 0xffu) {
+            uint2 e = make_uint2(t.gBase, t.gBits);
             if (t.sp < kStackSmem) sstack[t.sp * kTraceBlock + tid] = e;
             else if (t.sp < kStackSmem + kStackLocal) lstack[t.sp - kStackSmem] = e;
             else {
@@ -184,8 +195,10 @@ __device__ __forceinline__ bool trav_step(const Geom& s, Trav& t, uint2* sstack,
             atomicOr(errFlag, kErrBadIndex);
             return true;
         }
-        intersect_node(s.nodes, child, t.r, t.ix, t.iy, t.iz, t.octInv, t.tBest, t.gBase, t.tBase, t.gHits, t.gImask,
+        uint32_t hits, imask;
+        intersect_node(s.nodes, child, t.r, t.ix, t.iy, t.iz, t.octInv, t.tBest, t.gBase, t.tBase, hits, imask,
                        t.tMask);
+        t.gBits = hits | (imask << 8);
         if (t.tMask && t.tBase + (31u - __clz(t.tMask)) >= s.numTris) {
             atomicOr(errFlag, kErrBadIndex);
             return true;
@@ -197,28 +210,26 @@ __device__ __forceinline__ bool trav_step(const Geom& s, Trav& t, uint2* sstack,
         const float4* tp = s.tris + 3 * (size_t)(t.tBase + j);
         float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
         float th;
-        if (mt_rn(t.r, a, b, c, th) && th >= t.r.tmin && th <= t.r.tmax) {
-            uint32_t prim = __float_as_uint(a.w);
+        // closest hit: tBest <= tmax, so the update test below implies th <= tmax;
+        // any hit: tBest is tmax until the first hit, which ends the ray
+        if (mt_rn(t.r, a, b, c, th) && th >= t.r.tmin && (!kAnyHit || th <= t.tBest)) {
             if (kAnyHit) {
                 t.tBest = th;
-                t.pBest = prim;
+                t.lBest = t.tBase + j;
                 return true;
             }
-            if (th < t.tBest || (th == t.tBest && prim < t.pBest)) {
+            if (th < t.tBest || (th == t.tBest && __float_as_uint(a.w) < record_prim(s.tris, t.lBest))) {
                 t.tBest = th;
-                t.pBest = prim;
-                t.mBest = __float_as_uint(b.w);
                 t.lBest = t.tBase + j;
             }
         }
     }
-    if (!t.gHits) {
+    if (!(t.gBits & 0xffu)) {
         if (t.sp == 0) return true;
         --t.sp;
         uint2 e = t.sp < kStackSmem ? sstack[t.sp * kTraceBlock + tid] : lstack[t.sp - kStackSmem];
         t.gBase = e.x;
-        t.gHits = e.y & 0xffu;
-        t.gImask = e.y >> 8;
+        t.gBits = e.y;
     }
     return false;
 }
@@ -232,9 +243,9 @@ __device__ __forceinline__ bool traverse(const DevScene& s, const Ray& r, float&
     while (!trav_step<kAnyHit>(s, t, sstack, lstack, errFlag)) {
     }
     tBest = t.tBest;
-    pBest = t.pBest;
-    mBest = t.mBest;
-    return t.pBest != kNoHit;
+    pBest = record_prim(s.tris, t.lBest);
+    mBest = record_material(s.tris, t.lBest);
+    return t.lBest != kNoHit;
 }
 
 __device__ __forceinline__ Ray load_ray8(const float* p) {
@@ -300,16 +311,6 @@ __device__ __forceinline__ uint32_t warp_append_pos(uint32_t* counter, bool pred
     return pred ? pos : kInvalidSlot;
 }
 
-__device__ __forceinline__ uint32_t bucket_of(uint32_t type) {
-    switch (type) {
-        case kLambert: return kBucketLambert;
-        case kGlass:
-        case kGGXT: return kBucketDielectric;
-        case kGGX: return kBucketGGX;
-        default: return kBucketOther;
-    }
-}
-
 __device__ __forceinline__ PathQ pick_bucket(const Queues& q, uint32_t b) {
     switch (b) {
         case kBucketLambert: return q.bucket[kBucketLambert];
@@ -327,10 +328,19 @@ __device__ __forceinline__ PathQ pick_bucket(const Queues& q, uint32_t b) {
 #ifndef WRK_REFILL_AT
 #define WRK_REFILL_AT 16
 #endif
-#ifndef WRK_TRACE_MIN_BLOCKS
-#define WRK_TRACE_MIN_BLOCKS 8
+// Resident blocks per SM of each persistent trace kernel (its register budget is
+// 65536 / (128 x blocks)); the grid is that many blocks per SM.
+#ifndef WRK_TRACE_EXT_BLOCKS
+#define WRK_TRACE_EXT_BLOCKS 9
+#endif
+#ifndef WRK_TRACE_SHADOW_BLOCKS
+#define WRK_TRACE_SHADOW_BLOCKS 8
 #endif
 constexpr int kRefillAt = WRK_REFILL_AT;
+template <bool kAnyHit, bool kMulti>
+struct TraceBlocks {
+    static constexpr int value = kMulti ? 8 : (kAnyHit ? WRK_TRACE_SHADOW_BLOCKS : WRK_TRACE_EXT_BLOCKS);
+};
 
 // Adds a miss's environment term and accumulates the path into its request's sums
 // (__miss__trace + the raygen miss branch, trace.cu:143-148).
@@ -353,7 +363,8 @@ __device__ __forceinline__ void count_ended_t(SlotCtl* ctl, bool ended, uint32_t
 // kMulti: the batch's requests may use different scenes; a lane loads the
 // geometry of its ray's scene when it fetches the ray.  Otherwise scene s0.
 template <bool kAnyHit, bool kMulti>
-__global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_persistent(DevScene s0, Queues q) {
+__global__ void __launch_bounds__(kTraceBlock, (TraceBlocks<kAnyHit, kMulti>::value))
+    k_trace_persistent(DevScene s0, Queues q) {
     __shared__ uint2 sstack[kStackSmem * kTraceBlock];
     uint2 lstack[kStackLocal];
     Counters* c = q.ctr;
@@ -412,7 +423,7 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
             if (done) {
                 const float4 cc = in.sh_c[idx];
                 const uint32_t w = __float_as_uint(cc.w);
-                const bool lit = t.pBest == kNoHit;
+                const bool lit = t.lBest == kNoHit;
                 cont = w & 3u;
                 slot = __float_as_uint(in.sh_o[idx].w);
                 if (cont == kContExt) {
@@ -437,20 +448,20 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
             float4 th = make_float4(0, 0, 0, 0), rd = make_float4(0, 0, 0, 0);
             uint4 st = make_uint4(0, 0, 0, 0);
             bool missed = false;
+            uint32_t pBest = kNoHit, mBest = 0;
             if (done) {
                 th = in.thr[idx];
                 rd = in.rad[idx];
                 st = in.st[idx];
+                // prim, material and material bucket from the hit's record (just
+                // tested, so cached)
+                pBest = record_prim(geo.tris, t.lBest);
+                mBest = record_material(geo.tris, t.lBest);
                 const Frame& f = q.req[slot_of(st.w)];
-                if constexpr (kMulti) {
-                    const DevScene& sc = q.scenes[sceneIdx];
-                    if (t.pBest != kNoHit) bucket = t.mBest < sc.numMats ? bucket_of(sc.mats[t.mBest].type) : kBucketOther;
-                    else miss_accumulate(sc, f, th, rd, make_float3(t.r.dx, t.r.dy, t.r.dz));
-                } else {
-                    if (t.pBest != kNoHit) bucket = t.mBest < s0.numMats ? bucket_of(s0.mats[t.mBest].type) : kBucketOther;
-                    else miss_accumulate(s0, f, th, rd, make_float3(t.r.dx, t.r.dy, t.r.dz));
-                }
-                missed = t.pBest == kNoHit;
+                if (pBest != kNoHit) bucket = min(__float_as_uint(__ldg(geo.tris + 3 * (size_t)t.lBest + 2).w), (uint32_t)kBucketOther);
+                else if constexpr (kMulti) miss_accumulate(q.scenes[sceneIdx], f, th, rd, make_float3(t.r.dx, t.r.dy, t.r.dz));
+                else miss_accumulate(s0, f, th, rd, make_float3(t.r.dx, t.r.dy, t.r.dz));
+                missed = pBest == kNoHit;
             }
             count_ended_t(q.ctl, missed, slot_of(st.w));
             uint32_t pos = kInvalidSlot;
@@ -462,8 +473,8 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
             if (pos != kInvalidSlot) {
                 const PathQ o = pick_bucket(q, bucket);
                 o.ray_o[pos] = make_float4(t.r.ox, t.r.oy, t.r.oz, t.r.tmin);
-                o.ray_d[pos] = make_float4(t.r.dx, t.r.dy, t.r.dz, t.r.tmax);
-                o.hit[pos] = make_float4(t.tBest, __uint_as_float(t.pBest), __uint_as_float(t.mBest),
+                o.ray_d[pos] = make_float4(t.r.dx, t.r.dy, t.r.dz, t.tBest);
+                o.hit[pos] = make_float4(t.tBest, __uint_as_float(pBest), __uint_as_float(mBest),
                                          __uint_as_float(t.lBest));
                 o.thr[pos] = th;
                 o.rad[pos] = rd;
@@ -474,13 +485,13 @@ __global__ void __launch_bounds__(kTraceBlock, WRK_TRACE_MIN_BLOCKS) k_trace_per
     }
 }
 
-void launch_trace_extension(const DevScene& s, const Queues& q, bool multi, int grid, cudaStream_t st) {
-    if (multi) k_trace_persistent<false, true><<<grid, kTraceBlock, 0, st>>>(s, q);
-    else k_trace_persistent<false, false><<<grid, kTraceBlock, 0, st>>>(s, q);
+void launch_trace_extension(const DevScene& s, const Queues& q, bool multi, int numSMs, cudaStream_t st) {
+    if (multi) k_trace_persistent<false, true><<<numSMs * TraceBlocks<false, true>::value, kTraceBlock, 0, st>>>(s, q);
+    else k_trace_persistent<false, false><<<numSMs * TraceBlocks<false, false>::value, kTraceBlock, 0, st>>>(s, q);
 }
-void launch_trace_shadow(const DevScene& s, const Queues& q, bool multi, int grid, cudaStream_t st) {
-    if (multi) k_trace_persistent<true, true><<<grid, kTraceBlock, 0, st>>>(s, q);
-    else k_trace_persistent<true, false><<<grid, kTraceBlock, 0, st>>>(s, q);
+void launch_trace_shadow(const DevScene& s, const Queues& q, bool multi, int numSMs, cudaStream_t st) {
+    if (multi) k_trace_persistent<true, true><<<numSMs * TraceBlocks<true, true>::value, kTraceBlock, 0, st>>>(s, q);
+    else k_trace_persistent<true, false><<<numSMs * TraceBlocks<true, false>::value, kTraceBlock, 0, st>>>(s, q);
 }
 
 }  // namespace wrk

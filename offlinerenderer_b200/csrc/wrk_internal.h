@@ -45,6 +45,16 @@ enum : uint32_t {
     kBucketLambertResume = 4,
     kNumBuckets = 5
 };
+// The bucket of a material type; invalid material ids go to kBucketOther.
+__host__ __device__ inline uint32_t bucket_of_type(uint32_t type) {
+    switch (type) {
+        case kLambert: return kBucketLambert;
+        case kGlass:
+        case kGGXT: return kBucketDielectric;
+        case kGGX: return kBucketGGX;
+        default: return kBucketOther;
+    }
+}
 // st.w: flags in bits 0-7, the path's request slot in bits 8-15
 enum : uint32_t { kFlagFirstHit = 1u, kFlagPrevDelta = 2u };
 // What a Lambert path does after its shadow ray (sh_c.w): continue with the
@@ -95,13 +105,16 @@ struct DevScene {
     uint32_t numTris;
     float env[3];
     const uint4* nodes;
+    // BVH triangle records in leaf order, 3 float4 each: v0 | prim, v1 - v0 |
+    // material, v2 - v0 | bucket (the material's shade bucket, set at finalize)
     const float4* tris;
     uint32_t numNodes;
     const float4* envMap;  // lat-long RGBA f32 map (null = none); used with WRK_FLAG_ENV_MAP
     uint32_t envW, envH;
 };
 
-// One queue's entries, SoA.  Fields a queue does not carry are null.
+// One queue's entries, SoA.  Fields a queue does not carry are null.  ray_d.w is the
+// ray's tmax in the extension queues and the hit distance (hit.x) in the buckets.
 struct PathQ {
     float4* ray_o;
     float4* ray_d;
@@ -207,8 +220,9 @@ struct Queues {
 // scene up through its request); otherwise every request uses scene `s`.
 void launch_control(const Queues& q, cudaStream_t st);
 void launch_generate(const Queues& q, int grid, cudaStream_t st);
-void launch_trace_extension(const DevScene& s, const Queues& q, bool multi, int grid, cudaStream_t st);
-void launch_trace_shadow(const DevScene& s, const Queues& q, bool multi, int grid, cudaStream_t st);
+// persistent kernels: the grid is numSMs x the kernel's resident blocks per SM
+void launch_trace_extension(const DevScene& s, const Queues& q, bool multi, int numSMs, cudaStream_t st);
+void launch_trace_shadow(const DevScene& s, const Queues& q, bool multi, int numSMs, cudaStream_t st);
 void launch_shade_bucket(uint32_t bucket, const DevScene& s, const Queues& q, bool multi, int grid, int block,
                          cudaStream_t st);
 void launch_resolve(const Frame& f, uint32_t rawGuides, float* rgb, float* albedo, float* normal, cudaStream_t st);
@@ -232,6 +246,11 @@ int build_bvh8(const float* d_vtx, const uint32_t* d_idx, const uint32_t* d_triM
 
 // Sets the per-thread message returned by wrk_last_error(); returns `code`.
 int report_error(int code, const char* msg);
+
+// Writes the shade bucket of each BVH triangle record's material into its e2.w
+// (kernels_misc.cu).
+void launch_leaf_buckets(float4* tris, uint32_t numTris, const wrk_material* mats, uint32_t numMats,
+                         cudaStream_t st);
 
 // standalone ray queries (trace.cu)
 void launch_closest_query(const DevScene& s, const float* rays, uint32_t n, float* t, uint32_t* prim,

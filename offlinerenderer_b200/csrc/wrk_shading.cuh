@@ -62,8 +62,8 @@ __device__ __forceinline__ void frame(float3 n, float3& t, float3& b) {
 __device__ __forceinline__ float3 to_world(float3 v, float3 n, float3 t, float3 b) {
     return f3(t.x * v.x + b.x * v.y + n.x * v.z, t.y * v.x + b.y * v.y + n.y * v.z, t.z * v.x + b.z * v.y + n.z * v.z);
 }
-// sin / cos / pow of the sampling and Fresnel formulas, correctly rounded: CUDA's
-// double-precision functions rounded once to float.  The sampled directions and the
+// sin / cos / pow of the sampling and Fresnel formulas, correctly rounded: computed
+// in double precision and rounded once to float.  The sampled directions and the
 // VNDF pdf are sensitive to the last bit of these values (the GGX D term near its
 // peak multiplies an error of the half-vector by ~1/a^2), so the device rounds them
 // the one reproducible way; the oracle's matching mode does the same on the host.
@@ -73,7 +73,13 @@ __device__ __forceinline__ void sincos_cr(float x, float& s, float& c) {
     s = (float)sd;
     c = (float)cd;
 }
-__device__ __forceinline__ float pow_cr(float x, float y) { return (float)pow((double)x, (double)y); }
+// x^5 (the Schlick Fresnel power) in double: x^2 is exact, x^4 and x^5 carry one
+// double rounding each, so the float rounding is the correctly rounded x^5 except
+// when x^5 lies within ~2^-52 (relative) of a float rounding boundary.
+__device__ __forceinline__ float pow5_cr(float x) {
+    const double x2 = (double)x * (double)x;
+    return (float)(x2 * x2 * (double)x);
+}
 __device__ __forceinline__ float3 cosine_hemisphere(float u1, float u2, float& pdf) {
     float r = sqrtf(u1);
     float th = 2.0f * kPi * u2;
@@ -167,7 +173,7 @@ __device__ __forceinline__ float3 ggx_eval(float3 wo, float3 wi, float3 n, float
     f0 = f0 * f0;
     float3 F0 = f3(f0 * (1.0f - metal) + alb.x * metal, f0 * (1.0f - metal) + alb.y * metal,
                    f0 * (1.0f - metal) + alb.z * metal);
-    float fw = pow_cr(1.0f - voh, 5.0f);
+    float fw = pow5_cr(1.0f - voh);
     float3 F = f3(F0.x + (1.0f - F0.x) * fw, F0.y + (1.0f - F0.y) * fw, F0.z + (1.0f - F0.z) * fw);
     float den = 4.0f * nov * nol;
     float3 spec = f3(D * G * F.x / den, D * G * F.y / den, D * G * F.z / den);
