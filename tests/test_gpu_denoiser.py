@@ -46,6 +46,20 @@ def test_conv_forward_matches_torch(gpu, cin, cout):
     assert np.abs(y - ref).max() <= 2e-3 * scale, (np.abs(y - ref).max(), scale)
 
 
+@pytest.mark.parametrize("cin,cout,h,w", [(32, 32, 32, 80), (96, 32, 16, 16), (16, 48, 16, 48), (64, 16, 48, 16)])
+def test_conv_forward_tile_edges(gpu, cin, cout, h, w):
+    """Small-Cout layers (6-column output tiles): widths whose last tile in a row is
+    partial (80, 16) or exact (48), three output channel counts."""
+    rng = np.random.default_rng(cin + cout + h + w)
+    x = rng.standard_normal((1, h, w, cin)).astype(np.float32)
+    wt = (rng.standard_normal((cout, 3, 3, cin)) / np.sqrt(9 * cin)).astype(np.float32)
+    b = rng.standard_normal(cout).astype(np.float32)
+    y = gpu.conv3x3(x, wt, bias=b, relu=True, f32_out=True)
+    ref = _ref_conv(x, wt, b, relu=True)
+    scale = np.abs(ref).max()
+    assert np.abs(y - ref).max() <= 2e-3 * scale, (np.abs(y - ref).max(), scale)
+
+
 def test_conv_forward_relu_bf16_out(gpu):
     rng = np.random.default_rng(7)
     x = rng.standard_normal((1, 24, 48, 64)).astype(np.float32)
