@@ -44,58 +44,6 @@ constexpr uint32_t kTileW = 16, kTileH = 8, kTileP = 128;
 __host__ __device__ inline uint32_t round_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 
 // ---------------------------------------------------------------------------
-// Bias, ReLU, ReLU-derivative mask and store of 16 accumulated output channels
-// c0 .. c0 + 15 of one pixel.
-__device__ __forceinline__ void store16(const Epilogue& ep, size_t pix, uint32_t c0, float (&v)[16]) {
-    const uint32_t nv = min(16u, ep.coutValid - c0);
-#pragma unroll
-    for (uint32_t j = 0; j < 16; ++j) {
-        float x = v[j];
-        if (ep.bias && c0 + j < ep.nBias) x += ep.bias[c0 + j];
-        if (ep.relu) x = fmaxf(x, 0.0f);
-        v[j] = x;
-    }
-    if (ep.mask) {
-        const __nv_bfloat16* m = ep.mask + pix * ep.maskStride + ep.maskOffset + c0;
-#pragma unroll
-        for (uint32_t j = 0; j < 16; ++j)
-            if (j < nv && !(__bfloat162float(m[j]) > 0.0f)) v[j] = 0.0f;
-    }
-    if (ep.outF32) {
-        float* o = (float*)ep.out + pix * ep.outStride + ep.outOffset + c0;
-        if (nv == 16 && ((uintptr_t)o & 15u) == 0) {
-#pragma unroll
-            for (uint32_t j = 0; j < 16; j += 4) {
-                float4 x = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-                if (ep.accumulate) {
-                    float4 y = *(float4*)(o + j);
-                    x.x += y.x;
-                    x.y += y.y;
-                    x.z += y.z;
-                    x.w += y.w;
-                }
-                *(float4*)(o + j) = x;
-            }
-        } else {
-            for (uint32_t j = 0; j < nv; ++j) o[j] = ep.accumulate ? o[j] + v[j] : v[j];
-        }
-    } else {
-        __nv_bfloat16* o = (__nv_bfloat16*)ep.out + pix * ep.outStride + ep.outOffset + c0;
-        if (nv == 16 && ((uintptr_t)o & 15u) == 0) {
-            uint32_t p[8];
-#pragma unroll
-            for (uint32_t j = 0; j < 8; ++j) {
-                __nv_bfloat162 t = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
-                p[j] = *(uint32_t*)&t;
-            }
-            *(uint4*)o = make_uint4(p[0], p[1], p[2], p[3]);
-            *(uint4*)(o + 8) = make_uint4(p[4], p[5], p[6], p[7]);
-        } else {
-            for (uint32_t j = 0; j < nv; ++j) o[j] = __float2bfloat16_rn(v[j]);
-        }
-    }
-}
-
 // Epilogue of one 128-pixel tile: thread (warp w, lane l) owns TMEM lane / tile
 // row 32w + l and its N accumulator columns starting at `col`.
 __device__ __forceinline__ void fwd_epilogue(const FwdShape& sh, const Epilogue& ep, uint32_t tmem, uint32_t col,
@@ -108,7 +56,53 @@ __device__ __forceinline__ void fwd_epilogue(const FwdShape& sh, const Epilogue&
         float v[16];
         tmem_ld16(tmem + ((warp * 32u) << 16) + col + c0, v);
         if (c0 >= ep.coutValid) continue;
-        store16(ep, pix, c0, v);
+        const uint32_t nv = min(16u, ep.coutValid - c0);
+#pragma unroll
+        for (uint32_t j = 0; j < 16; ++j) {
+            float x = v[j];
+            if (ep.bias && c0 + j < ep.nBias) x += ep.bias[c0 + j];
+            if (ep.relu) x = fmaxf(x, 0.0f);
+            v[j] = x;
+        }
+        if (ep.mask) {
+            const __nv_bfloat16* m = ep.mask + pix * ep.maskStride + ep.maskOffset + c0;
+#pragma unroll
+            for (uint32_t j = 0; j < 16; ++j)
+                if (j < nv && !(__bfloat162float(m[j]) > 0.0f)) v[j] = 0.0f;
+        }
+        if (ep.outF32) {
+            float* o = (float*)ep.out + pix * ep.outStride + ep.outOffset + c0;
+            if (nv == 16 && ((uintptr_t)o & 15u) == 0) {
+#pragma unroll
+                for (uint32_t j = 0; j < 16; j += 4) {
+                    float4 x = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+                    if (ep.accumulate) {
+                        float4 y = *(float4*)(o + j);
+                        x.x += y.x;
+                        x.y += y.y;
+                        x.z += y.z;
+                        x.w += y.w;
+                    }
+                    *(float4*)(o + j) = x;
+                }
+            } else {
+                for (uint32_t j = 0; j < nv; ++j) o[j] = ep.accumulate ? o[j] + v[j] : v[j];
+            }
+        } else {
+            __nv_bfloat16* o = (__nv_bfloat16*)ep.out + pix * ep.outStride + ep.outOffset + c0;
+            if (nv == 16 && ((uintptr_t)o & 15u) == 0) {
+                uint32_t p[8];
+#pragma unroll
+                for (uint32_t j = 0; j < 8; ++j) {
+                    __nv_bfloat162 t = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+                    p[j] = *(uint32_t*)&t;
+                }
+                *(uint4*)o = make_uint4(p[0], p[1], p[2], p[3]);
+                *(uint4*)(o + 8) = make_uint4(p[4], p[5], p[6], p[7]);
+            } else {
+                for (uint32_t j = 0; j < nv; ++j) o[j] = __float2bfloat16_rn(v[j]);
+            }
+        }
     }
 }
 
@@ -422,188 +416,6 @@ __global__ void __launch_bounds__(192, 1)
 }
 
 // ---------------------------------------------------------------------------
-// Small-N variant with the three horizontal taps stacked along the MMA's N (3 x N
-// <= 256 accumulator columns).  The input block is 8 pixels wide and 16 rows high
-// (M = 128, TMEM lane = block pixel, a block row's 8 pixels in 8 adjacent lanes);
-// for each vertical tap dy and 16 input channels one M128 x N(3N) x K16
-// instruction forms D[p][dx * N + co] = sum_ci W[co][dy][dx][ci] X[p + dy rows][ci]
-// for all three dx at once, and the epilogue adds D[p - 1][dx = 0] + D[p][1] +
-// D[p + 1][2] with lane shuffles.  A block therefore outputs its inner 6 columns
-// (tiles step 6 pixels across; the last tile may be partial).  Per 16 input
-// channels that is three instructions of width 3N instead of nine of width N, so
-// the 4 KB A operand is read from shared memory three times instead of nine.  The
-// halo of a tile is 8 x 18 pixels ([channel group][row][8 pixels][8 channels],
-// 2304 bytes per group): rows are one core matrix apart (128 bytes) along M, and
-// the tap dy is an offset of dy rows into the same halo.
-constexpr uint32_t kRTileW = 6, kRBlockW = 8, kRHaloH = 18;
-constexpr uint32_t kRGroupBytes = kRBlockW * kRHaloH * 16;  // 2304, a multiple of 128
-
-__device__ __forceinline__ void rows_epilogue(const FwdShape& sh, const Epilogue& ep, uint32_t tmem, uint32_t col,
-                                              uint32_t warp, uint32_t lane, uint32_t b, uint32_t h0, uint32_t w0) {
-    const uint32_t row = warp * 32 + lane;
-    const uint32_t c = row % kRBlockW;  // block column; image column w0 + c - 1
-    const uint32_t h = h0 + row / kRBlockW, w = w0 + c - 1;
-    const bool valid = c >= 1 && c <= kRTileW && w < sh.W;
-    const size_t pix = ((size_t)b * sh.H + h) * sh.W + w;
-    const uint32_t taddr = tmem + ((warp * 32u) << 16) + col;
-    for (uint32_t c0 = 0; c0 < sh.N; c0 += 16) {
-        float l[16], m[16], r[16], v[16];
-        tmem_ld16(taddr + c0, l);
-        tmem_ld16(taddr + sh.N + c0, m);
-        tmem_ld16(taddr + 2 * sh.N + c0, r);
-#pragma unroll
-        for (uint32_t j = 0; j < 16; ++j)
-            v[j] = __shfl_up_sync(0xffffffffu, l[j], 1) + m[j] + __shfl_down_sync(0xffffffffu, r[j], 1);
-        if (c0 >= ep.coutValid || !valid) continue;
-        store16(ep, pix, c0, v);
-    }
-}
-
-template <int CIN>
-__global__ void __launch_bounds__(192, 1)
-    k_conv_fwd_rows(const __grid_constant__ CUtensorMap mh, const __nv_bfloat16* __restrict__ wgt, FwdShape sh,
-                    Epilogue ep, uint32_t* err) {
-    if (CIN > 0) sh.Cin = CIN;
-    extern __shared__ uint8_t smem_raw[];
-    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const uint32_t G = sh.Cin / 8;  // channel groups
-    const uint32_t N3 = 3 * sh.N;
-    const uint32_t haloBytes = G * kRGroupBytes;
-    const uint32_t stageBytes = round_up(haloBytes, 1024);
-    const uint32_t wBytes = round_up(9 * sh.Cin * sh.N * 2, 1024);
-    const uint32_t S = sh.stages;
-    uint8_t* wsm = smem + S * stageBytes;
-    uint64_t* bars = (uint64_t*)(wsm + wBytes);
-    uint32_t* tmemSlot = (uint32_t*)(bars + 2 * S + 5);
-    volatile uint32_t* abortFlag = tmemSlot + 1;
-    const uint32_t base = smem_u32(smem), wbase = smem_u32(wsm);
-    auto full = [&](uint32_t s) { return smem_u32(bars + s); };
-    auto empty = [&](uint32_t s) { return smem_u32(bars + S + s); };
-    auto accFull = [&](uint32_t b) { return smem_u32(bars + 2 * S + b); };
-    auto accEmpty = [&](uint32_t b) { return smem_u32(bars + 2 * S + 2 + b); };
-    const uint32_t drain = smem_u32(bars + 2 * S + 4);
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-
-    // weights -> shared memory, [dy][k group][dx * N + co][8 channels]
-    {
-        const uint32_t K = 9 * sh.Cin, units = 3 * G * N3;
-        for (uint32_t u = threadIdx.x; u < units; u += blockDim.x) {
-            const uint32_t n3 = u % N3, rest = u / N3, kg = rest % G, dy = rest / G;
-            const uint32_t dx = n3 / sh.N, co = n3 % sh.N;
-            const uint4 v =
-                *reinterpret_cast<const uint4*>(wgt + (size_t)(co + sh.wRow0) * K + (dy * 3 + dx) * sh.Cin + kg * 8);
-            *reinterpret_cast<uint4*>(wsm + (size_t)u * 16) = v;
-        }
-        fence_proxy_async();
-    }
-    if (threadIdx.x == 0) {
-        for (uint32_t s = 0; s < S; ++s) {
-            mbar_init(full(s), 1);
-            mbar_init(empty(s), 1);
-        }
-        for (uint32_t b = 0; b < 2; ++b) {
-            mbar_init(accFull(b), 1);
-            mbar_init(accEmpty(b), 128);
-        }
-        mbar_init(drain, 1);
-        *abortFlag = 0;
-        fence_mbar_init();
-        prefetch_map(&mh);
-    }
-    if (warp == 0) {
-        tmem_alloc(smem_u32(tmemSlot), sh.tmemCols);
-        tmem_relinquish();
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = *tmemSlot;
-
-    const uint32_t perImg = sh.tilesX * sh.tilesY;  // 6-column x 16-row output tiles
-    const uint32_t numTiles = sh.B * perImg;
-
-    if (warp == 4) {
-        if (lane == 0) {  // TMA producer: one 8 x 18 halo per tile
-            uint32_t it = 0, issued = 0;
-            for (uint32_t tile = blockIdx.x; tile < numTiles && !*abortFlag; tile += gridDim.x, ++it) {
-                const uint32_t s = it % S, round = it / S;
-                if (!mbar_wait(empty(s), (round & 1u) ^ 1u)) {
-                    *abortFlag = 1;
-                    break;
-                }
-                const uint32_t b = tile / perImg, rem = tile % perImg;
-                const int h0 = (int)((rem / sh.tilesX) * kHTileH), w0 = (int)((rem % sh.tilesX) * kRTileW);
-                mbar_expect_tx(full(s), haloBytes);
-                for (uint32_t g = 0; g < G; ++g)
-                    tma_load_4d(base + s * stageBytes + g * kRGroupBytes, &mh, full(s), (int)(g * 8), w0 - 1, h0 - 1,
-                                (int)b);
-                ++issued;
-            }
-            if (*abortFlag) {
-                for (uint32_t k = issued > S ? issued - S : 0; k < issued; ++k) mbar_wait(full(k % S), (k / S) & 1u);
-            }
-        }
-    } else if (warp == 5) {
-        if (lane == 0) {  // MMA issuer
-            const uint32_t idesc = idesc_bf16(N3, false, false);
-            const uint32_t lboA = kRGroupBytes, sboA = kRBlockW * 16;  // K step of 8 channels, M step of 8 pixels
-            const uint32_t lboB = N3 * 16, sboB = 8 * 16;
-            uint32_t it = 0;
-            for (uint32_t tile = blockIdx.x; tile < numTiles && !*abortFlag; tile += gridDim.x, ++it) {
-                const uint32_t buf = it & 1u, use = it >> 1;
-                const uint32_t s = it % S, round = it / S;
-                if (!mbar_wait(accEmpty(buf), (use & 1u) ^ 1u) || !mbar_wait(full(s), round & 1u)) {
-                    *abortFlag = 1;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t acc = tmem + buf * N3;
-                // descriptors advance by (byte offset >> 4) in their low 14-bit address field
-                const uint64_t a0 = sdesc(base + s * stageBytes, lboA, sboA, 0);
-                const uint64_t b0 = sdesc(wbase, lboB, sboB, 0);
-                constexpr uint32_t kKC = CIN > 0 ? CIN / 16 : 8;
-#pragma unroll
-                for (uint32_t dy = 0; dy < 3; ++dy) {
-#pragma unroll
-                    for (uint32_t kk = 0; kk < kKC; ++kk) {
-                        if (CIN == 0 && kk >= sh.Cin / 16) break;
-                        const uint64_t ad = a0 + (2 * kk * (kRGroupBytes >> 4) + dy * kRBlockW);
-                        const uint64_t bd = b0 + (dy * G + 2 * kk) * N3;
-                        umma_bf16(acc, ad, bd, idesc, (dy | kk) ? 1u : 0u);
-                    }
-                }
-                umma_commit(empty(s));
-                umma_commit(accFull(buf));
-            }
-            umma_commit(drain);
-            mbar_wait(drain, 0);
-        }
-    } else {
-        uint32_t it = 0;
-        for (uint32_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++it) {
-            const uint32_t buf = it & 1u, use = it >> 1;
-            const bool ready = mbar_wait(accFull(buf), use & 1u);
-            const bool go = __all_sync(0xffffffffu, ready && !*abortFlag);
-            tc_fence_after();
-            if (!go) {
-                *abortFlag = 1;
-                break;
-            }
-            const uint32_t b = tile / perImg, rem = tile % perImg;
-            rows_epilogue(sh, ep, tmem, buf * N3, warp, lane, b, (rem / sh.tilesX) * kHTileH,
-                          (rem % sh.tilesX) * kRTileW);
-            tc_fence_before();
-            mbar_arrive(accEmpty(buf));
-        }
-    }
-    __syncwarp();
-    tc_fence_before();
-    __syncthreads();
-    if (threadIdx.x == 0 && *abortFlag) atomicOr(err, 1u);
-    if (warp == 0) tmem_dealloc(tmem, sh.tmemCols);
-}
-
-// ---------------------------------------------------------------------------
 template <int CA, int CB>
 __global__ void __launch_bounds__(128, 1)
     k_conv_wgrad(const __grid_constant__ CUtensorMap mg, const __grid_constant__ CUtensorMap mx, WgradShape sh,
@@ -822,21 +634,13 @@ int plan_fwd(uint32_t B, uint32_t H, uint32_t W, uint32_t Cin, uint32_t N, uint3
     sh.stages = S;
     p->smem = smem_for(S * stage + (2 * S + 5) * 8 + 16 + 1024, sh.tmemCols);
     p->halo = false;
-    p->rows = false;
     const uint32_t wBytes = round_up(9 * Cin * N * 2, 1024);
     if (N <= 128 && wBytes <= 72u * 1024u && H % kHTileH == 0 && W % kHTileW == 0) {
         // small N: weights resident, one halo per 8 x 16 tile
         p->halo = true;
         sh.tilesX = W / kHTileW;
         sh.tilesY = H / kHTileH;
-        uint32_t hs = round_up(Cin / 8 * kHaloGroupBytes, 1024);
-        if (3 * N <= 256) {
-            // smaller still: the three horizontal taps share one instruction, 6 x 16 tiles
-            p->rows = true;
-            sh.tilesX = (W + kRTileW - 1) / kRTileW;
-            sh.tmemCols = pow2_cols(2 * 3 * N);
-            hs = round_up(Cin / 8 * kRGroupBytes, 1024);
-        }
+        const uint32_t hs = round_up(Cin / 8 * kHaloGroupBytes, 1024);
         uint32_t Sh = std::max(2u, std::min(4u, (200u * 1024u - wBytes) / hs));
         sh.stages = Sh;
         p->smem = smem_for(Sh * hs + wBytes + (2 * Sh + 5) * 8 + 16 + 1024, sh.tmemCols);
@@ -847,14 +651,13 @@ int plan_fwd(uint32_t B, uint32_t H, uint32_t W, uint32_t Cin, uint32_t N, uint3
     return 0;
 }
 
-static int make_halo_map(CUtensorMap* m, const void* base, uint32_t C, uint32_t W, uint32_t H, uint32_t B,
-                         uint32_t boxW, uint32_t boxH) {
+static int make_halo_map(CUtensorMap* m, const void* base, uint32_t C, uint32_t W, uint32_t H, uint32_t B) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return 1;
     if (((uintptr_t)base & 15u) || (C * 2) % 16) return 2;
     cuuint64_t dims[4] = {C, W, H, B};
     cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
-    cuuint32_t box[4] = {8, boxW, boxH, 1};
+    cuuint32_t box[4] = {8, kHaloW, kHaloH, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, es,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -864,8 +667,7 @@ static int make_halo_map(CUtensorMap* m, const void* base, uint32_t C, uint32_t 
 
 int make_input_map(const FwdPlan& p, const void* x, CUtensorMap* mx) {
     const FwdShape& sh = p.shape;
-    if (p.rows) return make_halo_map(mx, x, sh.Cin, sh.W, sh.H, sh.B, kRBlockW, kRHaloH);
-    if (p.halo) return make_halo_map(mx, x, sh.Cin, sh.W, sh.H, sh.B, kHaloW, kHaloH);
+    if (p.halo) return make_halo_map(mx, x, sh.Cin, sh.W, sh.H, sh.B);
     return make_act_map(mx, x, sh.Cin, sh.W, sh.H, sh.B, p.chunk);
 }
 
@@ -910,26 +712,6 @@ static cudaError_t set_smem(K kern, uint32_t bytes) {
 cudaError_t launch_fwd(const FwdPlan& p, const CUtensorMap& mx, const CUtensorMap& mw, const void* w,
                        const Epilogue& ep, uint32_t* err, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
-    if (p.rows) {
-        const __nv_bfloat16* wb = (const __nv_bfloat16*)w;
-#define WRK_ROWS_CASE(C)                                                                       \
-    case C:                                                                                    \
-        e = set_smem(k_conv_fwd_rows<C>, p.smem);                                             \
-        if (e == cudaSuccess) k_conv_fwd_rows<C><<<p.grid, 192, p.smem, st>>>(mx, wb, p.shape, ep, err); \
-        break;
-        switch (p.shape.Cin) {
-            WRK_ROWS_CASE(16)
-            WRK_ROWS_CASE(32)
-            WRK_ROWS_CASE(64)
-            WRK_ROWS_CASE(96)
-            default:
-                e = set_smem(k_conv_fwd_rows<0>, p.smem);
-                if (e == cudaSuccess) k_conv_fwd_rows<0><<<p.grid, 192, p.smem, st>>>(mx, wb, p.shape, ep, err);
-                break;
-        }
-#undef WRK_ROWS_CASE
-        return e != cudaSuccess ? e : cudaGetLastError();
-    }
     if (p.halo) {
         const __nv_bfloat16* wb = (const __nv_bfloat16*)w;
 #define WRK_HALO_CASE(C)                                                                       \

@@ -10,7 +10,7 @@ namespace conv {
 
 struct FwdShape {
     uint32_t B, H, W, Cin, N;  // N = output channels padded to a multiple of 16 (<= 256)
-    uint32_t tilesX, tilesY;   // output tiles (16 x 8 pixels; 8 x 16 halo; 6 x 16 rows)
+    uint32_t tilesX, tilesY;   // 16 x 8 pixel tiles
     uint32_t stages, tmemCols;
     uint32_t wRow0;            // first weight row (output channel) this launch computes
 };
@@ -42,7 +42,6 @@ struct FwdPlan {
     int chunk;
     uint32_t smem, grid;
     bool halo;  // small-N kernel: resident weights, one halo load per 8 x 16 tile
-    bool rows;  // halo variant with the horizontal taps stacked along N (3 x N <= 256), 6 x 16 tiles
 };
 struct WgradPlan {
     WgradShape shape;

@@ -48,8 +48,8 @@ def test_conv_forward_matches_torch(gpu, cin, cout):
 
 @pytest.mark.parametrize("cin,cout,h,w", [(32, 32, 32, 80), (96, 32, 16, 16), (16, 48, 16, 48), (64, 16, 48, 16)])
 def test_conv_forward_tile_edges(gpu, cin, cout, h, w):
-    """Small-Cout layers (6-column output tiles): widths whose last tile in a row is
-    partial (80, 16) or exact (48), three output channel counts."""
+    """Small-Cout layers at other image sizes: a single 16-pixel column, tall and wide
+    images, and 16 / 32 / 48 output channels."""
     rng = np.random.default_rng(cin + cout + h + w)
     x = rng.standard_normal((1, h, w, cin)).astype(np.float32)
     wt = (rng.standard_normal((cout, 3, 3, cin)) / np.sqrt(9 * cin)).astype(np.float32)
