@@ -170,6 +170,10 @@ Engine::~Engine() {
     if (hReq) cudaFreeHost(hReq);
     if (hGenOrder) cudaFreeHost(hGenOrder);
     if (hScenes) cudaFreeHost(hScenes);
+    if (side) cudaStreamSynchronize(side);
+    if (forkEv) cudaEventDestroy(forkEv);
+    if (joinEv) cudaEventDestroy(joinEv);
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -179,6 +183,12 @@ cudaError_t Engine::init(int dev, uint32_t cap) {
     capacity = std::max(cap ? cap : (1u << 22), 1024u);
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)) != cudaSuccess) return e;
+#ifndef WRK_NO_SHADOW_OVERLAP
+    if ((e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&forkEv, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&joinEv, cudaEventDisableTiming)) != cudaSuccess)
+        return e;
+#endif
     if ((e = cudaMallocHost(&hCtr, sizeof(Counters))) != cudaSuccess ||
         (e = cudaMallocHost(&hCtl, sizeof(SlotCtl) * kMaxSlots)) != cudaSuccess ||
         (e = cudaMallocHost(&hReq, sizeof(Frame) * kMaxSlots)) != cudaSuccess ||
@@ -256,6 +266,24 @@ cudaError_t Engine::reset_counters() {
 }
 
 static void launch_iteration(const Engine& E, const DevScene& s0, bool multi, cudaStream_t st, cudaEvent_t* ev) {
+    if (!ev && E.side) {
+        // captured chunk: the shadow trace (it reads this iteration's shadow queue and
+        // updates the continuations the last iteration left in the other extension
+        // buffer) overlaps generation and the extension trace (this iteration's
+        // extension buffer and the material buckets); the shade kernels wait for both
+        launch_control(E.q, st);
+        cudaEventRecord(E.forkEv, st);
+        cudaStreamWaitEvent(E.side, E.forkEv, 0);
+        launch_trace_shadow(s0, E.q, multi, E.numSMs, E.side);
+        cudaEventRecord(E.joinEv, E.side);
+        launch_generate(E.q, E.numSMs * 8, st);
+        launch_trace_extension(s0, E.q, multi, E.numSMs, st);
+        cudaStreamWaitEvent(st, E.joinEv, 0);
+        for (uint32_t b = 0; b < kNumBuckets; ++b)
+            if (b != kBucketLambertResume)
+                launch_shade_bucket(b, s0, E.q, multi, E.shade_grid(), (int)E.cfg.shadeBlock, st);
+        return;
+    }
     if (ev) cudaEventRecord(ev[0], st);
     launch_control(E.q, st);
     if (ev) cudaEventRecord(ev[1], st);

@@ -43,6 +43,12 @@ struct Engine {
     uint32_t capacity = 0;
     int numSMs = 148;
     cudaStream_t stream = nullptr;
+    // Inside a captured chunk the shadow trace of an iteration runs on `side`,
+    // concurrently with that iteration's camera-ray generation and extension trace
+    // (they touch disjoint queues), so each persistent kernel's tail is filled by
+    // the other; the shade kernels wait for both.
+    cudaStream_t side = nullptr;
+    cudaEvent_t forkEv = nullptr, joinEv = nullptr;
     EngineBuf queues, counters, tables;
     Queues q{};
     Frame* dReq = nullptr;
