@@ -171,9 +171,11 @@ Engine::~Engine() {
     if (hGenOrder) cudaFreeHost(hGenOrder);
     if (hScenes) cudaFreeHost(hScenes);
     if (side) cudaStreamSynchronize(side);
-    if (forkEv) cudaEventDestroy(forkEv);
-    if (joinEv) cudaEventDestroy(joinEv);
+    if (side2) cudaStreamSynchronize(side2);
+    for (cudaEvent_t e : {forkEv, joinEv, bucketsEv, join2Ev})
+        if (e) cudaEventDestroy(e);
     if (side) cudaStreamDestroy(side);
+    if (side2) cudaStreamDestroy(side2);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -185,8 +187,11 @@ cudaError_t Engine::init(int dev, uint32_t cap) {
     if ((e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)) != cudaSuccess) return e;
 #ifndef WRK_NO_SHADOW_OVERLAP
     if ((e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&side2, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&forkEv, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&joinEv, cudaEventDisableTiming)) != cudaSuccess)
+        (e = cudaEventCreateWithFlags(&joinEv, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&bucketsEv, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&join2Ev, cudaEventDisableTiming)) != cudaSuccess)
         return e;
 #endif
     if ((e = cudaMallocHost(&hCtr, sizeof(Counters))) != cudaSuccess ||
@@ -279,9 +284,14 @@ static void launch_iteration(const Engine& E, const DevScene& s0, bool multi, cu
         launch_generate(E.q, E.numSMs * 8, st);
         launch_trace_extension(s0, E.q, multi, E.numSMs, st);
         cudaStreamWaitEvent(st, E.joinEv, 0);
-        for (uint32_t b = 0; b < kNumBuckets; ++b)
-            if (b != kBucketLambertResume)
-                launch_shade_bucket(b, s0, E.q, multi, E.shade_grid(), (int)E.cfg.shadeBlock, st);
+        // the small buckets' shade kernels beside the Lambert shade
+        cudaEventRecord(E.bucketsEv, st);
+        cudaStreamWaitEvent(E.side2, E.bucketsEv, 0);
+        for (uint32_t b : {kBucketDielectric, kBucketGGX, kBucketOther})
+            launch_shade_bucket(b, s0, E.q, multi, E.shade_grid(), (int)E.cfg.shadeBlock, E.side2);
+        cudaEventRecord(E.join2Ev, E.side2);
+        launch_shade_bucket(kBucketLambert, s0, E.q, multi, E.shade_grid(), (int)E.cfg.shadeBlock, st);
+        cudaStreamWaitEvent(st, E.join2Ev, 0);
         return;
     }
     if (ev) cudaEventRecord(ev[0], st);

@@ -49,6 +49,10 @@ struct Engine {
     // the other; the shade kernels wait for both.
     cudaStream_t side = nullptr;
     cudaEvent_t forkEv = nullptr, joinEv = nullptr;
+    // likewise the glass, GGX and emissive shade kernels run on `side2`, concurrently
+    // with the Lambert shade (each reads its own bucket; their appends are atomic)
+    cudaStream_t side2 = nullptr;
+    cudaEvent_t bucketsEv = nullptr, join2Ev = nullptr;
     EngineBuf queues, counters, tables;
     Queues q{};
     Frame* dReq = nullptr;
