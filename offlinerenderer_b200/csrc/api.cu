@@ -851,6 +851,7 @@ static int render_impl(wrk_renderer* r, wrk_scene* s, const wrk_camera* cam, con
         stats->shadowRays = h.shdRays + h.shadowAnswered.v;  // + the last iteration's answered queries
         stats->shadowTraced = h.shdTraced;
         for (int b = 0; b < kNumBuckets; ++b) stats->bucketPaths[b] = h.bucketTotal[b] + h.bucket[b].v;
+        stats->bucketPaths[kBucketLambert] += h.lambertTex.v;
         stats->iterations = iters;
         stats->deviceErrors = h.error;
         cudaEventElapsedTime(&stats->gpuMs, r->evLoop0, r->evLoop1);

@@ -210,7 +210,7 @@ __global__ void k_tonemap(const float* __restrict__ rgb, uint32_t nfloat, uint8_
 __global__ void k_leaf_buckets(float4* tris, uint32_t nt, const wrk_material* __restrict__ mats, uint32_t numMats) {
     for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nt; l += gridDim.x * blockDim.x) {
         const uint32_t mat = __float_as_uint(tris[3 * (size_t)l + 1].w);
-        const uint32_t b = mat < numMats ? bucket_of_type(mats[mat].type) : (uint32_t)kBucketOther;
+        const uint32_t b = mat < numMats ? bucket_of_material(mats[mat]) : (uint32_t)kBucketOther;
         tris[3 * (size_t)l + 2].w = __uint_as_float(b);
     }
 }

@@ -67,6 +67,8 @@ __device__ __forceinline__ unsigned long long global_ns() {
 __global__ void k_control(Queues q) {
     Counters* c = q.ctr;
     for (int b = 0; b < kNumBuckets; ++b) c->bucketTotal[b] += c->bucket[b].v;
+    c->bucketTotal[kBucketLambert] += c->lambertTex.v;
+    c->lambertTex.v = 0;
     uint32_t cur = c->cur ^ 1u;
     uint32_t out = cur ^ 1u;
     c->cur = cur;
@@ -616,19 +618,24 @@ template <uint32_t kBucket, bool kMulti, int kBlock>
 __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k_shade(DevScene s0, Queues q) {
     Counters* c = q.ctr;
     const uint32_t cur = c->cur, nxt = cur ^ 1u;
+    // the Lambert queue holds plain hits at [0, n) and textured ones at the far end,
+    // [capacity - nt, capacity): threads take the plain ones first
     const uint32_t n = min(c->bucket[kBucket].v, q.capacity);
+    const uint32_t nt = kBucket == kBucketLambert ? min(c->lambertTex.v, q.capacity - n) : 0u;
+    const uint32_t total = n + nt;
     const PathQ in = q.bucket[kBucket];
     const PathQ ext = nxt ? q.ext[1] : q.ext[0];
     const PathQ shd = nxt ? q.shd[1] : q.shd[0];
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t i = base + threadIdx.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+        const uint32_t t = base + threadIdx.x;
+        const uint32_t i = t < n ? t : q.capacity - 1u - (t - n);
         PathRegs r;
         ShadowOut so;
         so.cont = kContDrop;
         so.answered = false;
         int out = kOutNone;
         uint32_t slot = 0;
-        if (i < n) {
+        if (t < total) {
             float4 o4 = in.ray_o[i], d4 = in.ray_d[i], h4 = in.hit[i], t4 = in.thr[i], r4 = in.rad[i];
             uint4 st = in.st[i];
             slot = slot_of(st.w);

@@ -458,17 +458,24 @@ __global__ void __launch_bounds__(kTraceBlock, (TraceBlocks<kAnyHit, kMulti>::va
                 pBest = record_prim(geo.tris, t.lBest);
                 mBest = record_material(geo.tris, t.lBest);
                 const Frame& f = q.req[slot_of(st.w)];
-                if (pBest != kNoHit) bucket = min(__float_as_uint(__ldg(geo.tris + 3 * (size_t)t.lBest + 2).w), (uint32_t)kBucketOther);
+                if (pBest != kNoHit) bucket = __float_as_uint(__ldg(geo.tris + 3 * (size_t)t.lBest + 2).w);
                 else if constexpr (kMulti) miss_accumulate(q.scenes[sceneIdx], f, th, rd, make_float3(t.r.dx, t.r.dy, t.r.dz));
                 else miss_accumulate(s0, f, th, rd, make_float3(t.r.dx, t.r.dy, t.r.dz));
                 missed = pBest == kNoHit;
             }
             count_ended_t(q.ctl, missed, slot_of(st.w));
+            // textured Lambert hits fill the Lambert queue from its last entry down
+            const bool texL = bucket == (kBucketLambert | kRecTextured);
+            if (bucket != kNumBuckets) bucket = texL ? (uint32_t)kBucketLambert : min(bucket, (uint32_t)kBucketOther);
             uint32_t pos = kInvalidSlot;
 #pragma unroll
             for (uint32_t b = 0; b < kBucketLambertResume; ++b) {
-                uint32_t pb = warp_append_pos(&c->bucket[b].v, bucket == b, q.capacity, &c->error);
-                if (bucket == b) pos = pb;
+                uint32_t pb = warp_append_pos(&c->bucket[b].v, bucket == b && !texL, q.capacity, &c->error);
+                if (bucket == b && !texL) pos = pb;
+            }
+            {
+                const uint32_t pt = warp_append_pos(&c->lambertTex.v, texL, q.capacity, &c->error);
+                if (texL && pt != kInvalidSlot) pos = q.capacity - 1u - pt;
             }
             if (pos != kInvalidSlot) {
                 const PathQ o = pick_bucket(q, bucket);

@@ -55,6 +55,15 @@ __host__ __device__ inline uint32_t bucket_of_type(uint32_t type) {
         default: return kBucketOther;
     }
 }
+// A leaf record's bucket word also flags Lambert materials with an albedo or normal
+// texture: their hits go to the far end of the Lambert queue (filled downward from the
+// last entry), so the shade kernel's warps see plain and textured hits apart and only
+// the textured ones take the texture fetches.
+constexpr uint32_t kRecTextured = 8u;
+__host__ __device__ inline uint32_t bucket_of_material(const wrk_material& m) {
+    const uint32_t b = bucket_of_type(m.type);
+    return b == kBucketLambert && (m.albedoTextureId != 0 || m.normalTextureId != 0) ? b | kRecTextured : b;
+}
 // st.w: flags in bits 0-7, the path's request slot in bits 8-15
 enum : uint32_t { kFlagFirstHit = 1u, kFlagPrevDelta = 2u };
 // What a Lambert path does after its shadow ray (sh_c.w): continue with the
@@ -142,6 +151,7 @@ struct Counters {
     HotCounter ext[2];
     HotCounter shd[2];
     HotCounter bucket[kNumBuckets];
+    HotCounter lambertTex;      // textured Lambert hits, stored from the Lambert queue's last entry down
     HotCounter cont;            // Lambert continuations placed in ext[cur] this iteration
     HotCounter contDirect;      // ... of them without a shadow entry (query answered in the shade)
     HotCounter shadowAnswered;  // shadow queries the Lambert shade answered this iteration
