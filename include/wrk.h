@@ -162,8 +162,9 @@ int wrk_scene_light_cdf(wrk_scene* s, uint32_t* tris, float* cdf, uint32_t capac
 /* Copies the 8-wide BVH to host memory for inspection: nodes = numNodes * 20 u32
  * (five 16-byte words each), tris = numTriangles * 12 floats (v0|prim, e1|material,
  * e2|bucket per triangle, in leaf order; bucket = the material's shade queue: 0
- * Lambert, 1 glass / rough glass, 2 GGX, 3 emissive or other, as a u32).  Sizes come
- * from wrk_scene_bvh_info. */
+ * Lambert, 1 glass / rough glass, 2 GGX, 3 emissive or other, plus 8 for a Lambert
+ * material with an albedo or normal texture, as a u32).  Sizes come from
+ * wrk_scene_bvh_info. */
 int wrk_scene_bvh_export(wrk_scene* s, uint32_t* nodes, float* tris);
 
 /* Device addresses of a finalized scene's buffers: the getters of wr::Scene
