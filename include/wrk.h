@@ -243,8 +243,10 @@ int wrk_server_result_device(wrk_server* s, uint64_t ticket, float* d_rgb, float
                              wrk_request_info* info);
 
 /* ---- autotuner: no counterpart in libWR.  Times one render of the given
- *      workload per launch shape (capacity 1M/2M/4M x chunk 4/8/16 x shading
- *      block 128/256) and returns the fastest. ---- */
+ *      workload per launch shape (capacity 1M/4M/16M/32M/64M paths x chunk 4/8/16
+ *      x shading block 128/256) and returns the fastest.  Capacities from 4M up are
+ *      tried only while their queues (672 bytes per path) plus 512 MB fit in the
+ *      device's free memory, so numTrials is 6 to 30. ---- */
 typedef struct {
     uint32_t capacity, chunk, shadeBlock;
     float ms;

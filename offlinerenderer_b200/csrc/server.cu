@@ -442,7 +442,10 @@ int wrk_server_result_device(wrk_server* sv, uint64_t ticket, float* d_rgb, floa
 int wrk_autotune(int device, wrk_scene* s, const wrk_camera* cam, const wrk_render_params* p, wrk_tune_result* out) {
     if (!s || !cam || !p || !out) return sfail(WRK_ERR_INVALID, "null argument");
     *out = wrk_tune_result{};
-    const uint32_t caps[3] = {1u << 20, 1u << 21, 1u << 22};
+    // queue capacities up to 64M paths (672 B each: 45 GB; a 512x512 frame at 256 spp
+    // then runs all its paths at once, in the 8 iterations a path may take); a capacity
+    // whose queues do not fit in the free device memory ends the search
+    const uint32_t caps[5] = {1u << 20, 1u << 22, 1u << 24, 1u << 25, 1u << 26};
     const uint32_t chunks[3] = {4, 8, 16};
     const uint32_t blocks[2] = {128, 256};
     const size_t np = (size_t)p->width * p->height;
@@ -451,8 +454,12 @@ int wrk_autotune(int device, wrk_scene* s, const wrk_camera* cam, const wrk_rend
     SCK(cudaMalloc(&d, np * 9 * sizeof(float)));
     int rc = WRK_OK;
     out->bestMs = 3.4e38f;
-    for (uint32_t ci = 0; ci < 3 && !rc; ++ci) {
+    for (uint32_t ci = 0; ci < 5 && !rc; ++ci) {
         wrk_renderer* r = nullptr;
+        size_t freeB = 0, totalB = 0;
+        if (ci > 0 && cudaMemGetInfo(&freeB, &totalB) == cudaSuccess &&
+            (size_t)caps[ci] * 672 + (size_t)512 * 1024 * 1024 > freeB)
+            break;
         if ((rc = wrk_renderer_create(device, caps[ci], &r))) break;
         for (uint32_t k = 0; k < 3 && !rc; ++k)
             for (uint32_t b = 0; b < 2 && !rc; ++b) {
