@@ -356,6 +356,9 @@ def main():
     ap.add_argument("--serve-ref-spp", type=int, default=1024,
                     help="spp of the FP64 references the served images are scored against")
     ap.add_argument("--ref-spp", type=int, default=4096)
+    ap.add_argument("--capacity", type=int, default=0,
+                    help="fixed queue capacity, chunk 8, 256-thread shading (skips the autotuner; small "
+                         "profiling cases)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
@@ -389,7 +392,10 @@ def main():
     # project's autotuner on this workload itself (at its full spp: the largest queue
     # capacities pay off only when the frame's paths fill them), outside the timed region
     # (rank 0 tunes and every rank uses its choice, so the ranks run the same shape)
-    tune = wrk.autotune(scene, spp=st.spp, device=local) if rank == 0 else None
+    if args.capacity:
+        tune = {"capacity": args.capacity, "chunk": 8, "shadeBlock": 256, "bestMs": None}
+    else:
+        tune = wrk.autotune(scene, spp=st.spp, device=local) if rank == 0 else None
     if dist is not None:
         box = [tune]
         dist.broadcast_object_list(box, src=0)
