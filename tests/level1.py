@@ -1,4 +1,4 @@
-"""The level-1 bound (north star): every finite BSDF / sampling / MIS output within
+"""The level-1 parity bound: every finite BSDF / sampling / MIS output within
 1e-5 relative of the FP64 transcription of the reference's formulas.  Shared by the
 GPU kernel tests and the CPU check of the reference's own FP32 outputs.
 

@@ -107,7 +107,7 @@ def test_bsdf_fp32_vs_oracle(gpu, oracle):
 
 
 def test_bsdf_vs_fp64_transcription(gpu, oracle):
-    """North-star level 1: the maximum (not a percentile) relative error against
+    """Parity level 1: the maximum (not a percentile) relative error against
     the FP64 transcription over every well-conditioned finite record is below
     1e-5, for every output column."""
     import pyoracle

@@ -1,4 +1,4 @@
-"""Whole-image parity (north-star level 3) and renderer behaviour on the GPU.
+"""Whole-image parity (parity level 3) and renderer behaviour on the GPU.
 
 The GPU renderer and the oracle draw the same random numbers for each (pixel,
 sample), so at equal seed and spp their images agree far inside the estimator's
@@ -141,7 +141,7 @@ def test_convergence_to_high_spp(gpu):
 
 
 def test_gpu_and_oracle_converge_to_one_fp64_reference(gpu, oracle):
-    """North-star level 3, second half: the GPU renderer and the oracle converge to
+    """Parity level 3, second half: the GPU renderer and the oracle converge to
     the same FP64-accumulated 4096-spp image.  The reference is the GPU's (f32 sums
     per 512-spp chunk accumulated in float64, sample indices from 2^20 on, disjoint
     from the others); the oracle's own 4096-spp render is as close to it as a second

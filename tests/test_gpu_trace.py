@@ -2,7 +2,7 @@
 
 Against the oracle's FP32 Moller-Trumbore (same arithmetic): primitive ids and t
 agree exactly.  Against the FP64 exact intersector: primitive ids agree on
->= 99.99% of rays and t within 1e-5 relative wherever both hit (north-star level
+>= 99.99% of rays and t within 1e-5 relative wherever both hit (parity level
 2).  The exact intersector tests every triangle in FP64 (oracle mode 1); on the
 2.41M-triangle scale scene it reaches the triangles by walking the oracle's CPU
 BVH with conservatively widened FP64 boxes (mode 2, checked equal to mode 1).
