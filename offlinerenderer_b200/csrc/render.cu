@@ -636,8 +636,11 @@ __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k
         int out = kOutNone;
         uint32_t slot = 0;
         if (t < total) {
-            float4 o4 = in.ray_o[i], d4 = in.ray_d[i], h4 = in.hit[i], t4 = in.thr[i], r4 = in.rad[i];
-            uint4 st = in.st[i];
+            // queue fields are read once: streaming loads keep L1 for materials,
+            // textures, triangle and light records
+            float4 o4 = __ldcs(in.ray_o + i), d4 = __ldcs(in.ray_d + i), h4 = __ldcs(in.hit + i), t4 = __ldcs(in.thr + i),
+                   r4 = __ldcs(in.rad + i);
+            uint4 st = __ldcs(in.st + i);
             slot = slot_of(st.w);
             const Frame& f = q.req[slot];
             if constexpr (kMulti) {

@@ -294,7 +294,9 @@ void launch_occluded_query(const DevScene& s, const float* rays, uint32_t n, uin
 // from the input queue entry it fetched and, when the ray is done, copies the
 // whole entry into the next queue at the position a warp-aggregated append (one
 // ballot per destination, one atomicAdd by the lowest lane) handed out, so the
-// lanes of a warp write consecutive entries.
+// lanes of a warp write consecutive entries.  Queue entries are read and written
+// once per pass, so they go through the cache with the streaming (evict-first)
+// policy (__ldcs / __stcs) and leave L1 to the BVH nodes and triangle records.
 __device__ __forceinline__ uint32_t warp_append_pos(uint32_t* counter, bool pred, uint32_t cap, uint32_t* err) {
     uint32_t b = __ballot_sync(0xffffffffu, pred);
     if (!b) return kInvalidSlot;
@@ -389,10 +391,10 @@ __global__ void __launch_bounds__(kTraceBlock, (TraceBlocks<kAnyHit, kMulti>::va
             if (!active && !exhausted) {
                 idx = base + __popc(idle & ((1u << lane) - 1u));
                 if (idx < n) {
-                    float4 o = kAnyHit ? in.sh_o[idx] : in.ray_o[idx];
-                    float4 d = kAnyHit ? in.sh_d[idx] : in.ray_d[idx];
+                    float4 o = kAnyHit ? __ldcs(in.sh_o + idx) : __ldcs(in.ray_o + idx);
+                    float4 d = kAnyHit ? __ldcs(in.sh_d + idx) : __ldcs(in.ray_d + idx);
                     // a shadow entry keeps its request slot where tmin would be
-                    const uint32_t slot = kAnyHit ? __float_as_uint(o.w) : slot_of(in.st[idx].w);
+                    const uint32_t slot = kAnyHit ? __float_as_uint(o.w) : slot_of(__ldcs(&in.st[idx].w));
                     if (kAnyHit) o.w = kShadowTmin;
                     if constexpr (kMulti) {
                         sceneIdx = q.req[slot].scene;
@@ -421,7 +423,7 @@ __global__ void __launch_bounds__(kTraceBlock, (TraceBlocks<kAnyHit, kMulti>::va
             // with the prepared extension ray, accumulate, or drop.
             uint32_t cont = kContDrop, slot = 0;
             if (done) {
-                const float4 cc = in.sh_c[idx];
+                const float4 cc = __ldcs(in.sh_c + idx);
                 const uint32_t w = __float_as_uint(cc.w);
                 const bool lit = t.lBest == kNoHit;
                 cont = w & 3u;
@@ -450,9 +452,9 @@ __global__ void __launch_bounds__(kTraceBlock, (TraceBlocks<kAnyHit, kMulti>::va
             bool missed = false;
             uint32_t pBest = kNoHit, mBest = 0;
             if (done) {
-                th = in.thr[idx];
-                rd = in.rad[idx];
-                st = in.st[idx];
+                th = __ldcs(in.thr + idx);
+                rd = __ldcs(in.rad + idx);
+                st = __ldcs(in.st + idx);
                 // prim, material and material bucket from the hit's record (just
                 // tested, so cached)
                 pBest = record_prim(geo.tris, t.lBest);
@@ -479,13 +481,13 @@ __global__ void __launch_bounds__(kTraceBlock, (TraceBlocks<kAnyHit, kMulti>::va
             }
             if (pos != kInvalidSlot) {
                 const PathQ o = pick_bucket(q, bucket);
-                o.ray_o[pos] = make_float4(t.r.ox, t.r.oy, t.r.oz, t.r.tmin);
-                o.ray_d[pos] = make_float4(t.r.dx, t.r.dy, t.r.dz, t.tBest);
+                __stcs(o.ray_o + pos, make_float4(t.r.ox, t.r.oy, t.r.oz, t.r.tmin));
+                __stcs(o.ray_d + pos, make_float4(t.r.dx, t.r.dy, t.r.dz, t.tBest));
                 o.hit[pos] = make_float4(t.tBest, __uint_as_float(pBest), __uint_as_float(mBest),
                                          __uint_as_float(t.lBest));
-                o.thr[pos] = th;
-                o.rad[pos] = rd;
-                o.st[pos] = st;
+                __stcs(o.thr + pos, th);
+                __stcs(o.rad + pos, rd);
+                __stcs(o.st + pos, st);
             }
         }
         if (done) active = false;
