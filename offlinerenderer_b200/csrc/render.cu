@@ -211,11 +211,11 @@ __global__ void __launch_bounds__(kShadeBlock) k_generate(Queues q) {
             ro = f3(pos.x + off.x, pos.y + off.y, pos.z + off.z);
             rd = normalize(f3(fp.x - ro.x, fp.y - ro.y, fp.z - ro.z));
         }
-        o.ray_o[e] = make_float4(ro.x, ro.y, ro.z, 0.0001f);
-        o.ray_d[e] = make_float4(rd.x, rd.y, rd.z, 1e20f);
-        o.thr[e] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-        o.rad[e] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(pixel));
-        o.st[e] = make_uint4(seed, 0u, 0u, kFlagFirstHit | kFlagPrevDelta | (sg.slot << kSlotShift));
+        __stcs(o.ray_o + e, make_float4(ro.x, ro.y, ro.z, 0.0001f));
+        __stcs(o.ray_d + e, make_float4(rd.x, rd.y, rd.z, 1e20f));
+        __stcs(o.thr + e, make_float4(1.0f, 1.0f, 1.0f, 1.0f));
+        __stcs(o.rad + e, make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(pixel)));
+        __stcs(o.st + e, make_uint4(seed, 0u, 0u, kFlagFirstHit | kFlagPrevDelta | (sg.slot << kSlotShift)));
     }
 }
 
@@ -670,24 +670,25 @@ __global__ void __launch_bounds__(kBlock, WRK_SHADE_MIN_BLOCKS * 256 / kBlock) k
                 if (direct) atomicAdd(&c->contDirect.v, (uint32_t)__popc(direct));
             }
         }
+        // entries are written once and read in a later pass: streaming stores
         if (pe != kInvalidSlot || pc != kInvalidSlot) {
             const PathQ o = pe != kInvalidSlot ? ext : (cur ? q.ext[1] : q.ext[0]);
             const uint32_t p = pe != kInvalidSlot ? pe : pc;
-            o.ray_o[p] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
-            o.ray_d[p] = make_float4(r.d.x, r.d.y, r.d.z, 1e20f);
-            o.thr[p] = make_float4(r.thr.x, r.thr.y, r.thr.z, r.prevPdf);
-            o.rad[p] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
-            o.st[p] = make_uint4(r.seed, r.dim, (r.depth & 0xffffu) | (r.iter << 16), r.flags);
+            __stcs(o.ray_o + p, make_float4(r.o.x, r.o.y, r.o.z, 0.0f));
+            __stcs(o.ray_d + p, make_float4(r.d.x, r.d.y, r.d.z, 1e20f));
+            __stcs(o.thr + p, make_float4(r.thr.x, r.thr.y, r.thr.z, r.prevPdf));
+            __stcs(o.rad + p, make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel)));
+            __stcs(o.st + p, make_uint4(r.seed, r.dim, (r.depth & 0xffffu) | (r.iter << 16), r.flags));
         }
         if (ps != kInvalidSlot) {
             // sh_o.w: the request slot (every shadow ray starts at kShadowTmin);
             // sh_c.w: the continuation code | the continuing path's position << 2
             uint32_t w = so.cont;
             if (cx) w = pc == kInvalidSlot ? (uint32_t)kContDrop : kContExt | (pc << 2);
-            if (so.cont == kContAccumulate) shd.rad[ps] = make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel));
-            shd.sh_o[ps] = make_float4(so.o.x, so.o.y, so.o.z, __uint_as_float(slot));
-            shd.sh_d[ps] = make_float4(so.d.x, so.d.y, so.d.z, so.dist - kShadowTmin);
-            shd.sh_c[ps] = make_float4(so.c.x, so.c.y, so.c.z, __uint_as_float(w));
+            if (so.cont == kContAccumulate) __stcs(shd.rad + ps, make_float4(r.rad.x, r.rad.y, r.rad.z, __uint_as_float(r.pixel)));
+            __stcs(shd.sh_o + ps, make_float4(so.o.x, so.o.y, so.o.z, __uint_as_float(slot)));
+            __stcs(shd.sh_d + ps, make_float4(so.d.x, so.d.y, so.d.z, so.dist - kShadowTmin));
+            __stcs(shd.sh_c + ps, make_float4(so.c.x, so.c.y, so.c.z, __uint_as_float(w)));
         }
     }
 }
