@@ -464,16 +464,19 @@ def main():
     stage_gbs = {k: (STAGE_BYTES[k] * units[k] / (stage_ms[k] / 1e3) / 1e9 if stage_ms[k] > 0 else None)
                  for k in STAGE_BYTES}
 
-    # end to end through the public C ABI with host buffers (one untimed call first:
-    # the renderer allocates its device staging for host output on first use)
+    # end to end through the public C ABI with host buffers: caller-owned pinned host
+    # arrays receive rgb, albedo and normal every step (one untimed call first: the
+    # renderer allocates its device staging for host output on first use)
     e2e_steps = max(1, min(args.steps, 5))
-    rend.render(scene, sample_offset=(999 * world + rank) * st.spp)
+    pinned = [torch.empty((st.height, st.width, 3), dtype=torch.float32).pin_memory() for _ in range(3)]
+    host = [t.numpy() for t in pinned]
+    rend.render(scene, sample_offset=(999 * world + rank) * st.spp, out=host)
     torch.cuda.synchronize()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
     e2.record()
     for i in range(e2e_steps):
-        rend.render(scene, sample_offset=(1000 + i * world + rank) * st.spp)
+        rend.render(scene, sample_offset=(1000 + i * world + rank) * st.spp, out=host)
     e3.record()
     torch.cuda.synchronize()
     e2e_ms = e2.elapsed_time(e3)

@@ -440,16 +440,29 @@ class Renderer:
         _check(lib().wrk_renderer_set_launch(self.handle, chunk, shade_block))
 
     def render(self, scene: Scene, camera=None, settings=None, spp=None, guides=True, raw_guides=False,
-               max_iterations=8, seed=None, sample_offset=0, stage_timing=False, env_map=False) -> RenderResult:
-        """Synchronous render into host buffers (rgb = sum/spp, as libWR returns it)."""
+               max_iterations=8, seed=None, sample_offset=0, stage_timing=False, env_map=False,
+               out=None) -> RenderResult:
+        """Synchronous render into host buffers (rgb = sum/spp, as libWR returns it).
+
+        out: optional (rgb, albedo, normal) float32 C-contiguous (height, width, 3)
+        arrays to write into (albedo / normal may be None when guides is False), as
+        libWR's caller-owned output buffer; pinned host memory makes the copy faster."""
         cam = camera_struct(camera or scene._data.camera)
         st = settings or scene._data.settings
         p = params_struct(st, spp=spp, max_iterations=max_iterations, raw_guides=raw_guides, seed=seed,
                           sample_offset=sample_offset, stage_timing=stage_timing, env_map=env_map)
         shape = (st.height, st.width, 3)
-        rgb = np.zeros(shape, np.float32)
-        alb = np.zeros(shape, np.float32) if guides else None
-        nrm = np.zeros(shape, np.float32) if guides else None
+        if out is not None:
+            rgb, alb, nrm = out
+            for a in (rgb, alb, nrm):
+                if a is not None and (a.shape != shape or a.dtype != np.float32 or not a.flags["C_CONTIGUOUS"]):
+                    raise ValueError(f"output arrays must be float32, C-contiguous, shape {shape}")
+            if not guides:
+                alb = nrm = None
+        else:
+            rgb = np.zeros(shape, np.float32)
+            alb = np.zeros(shape, np.float32) if guides else None
+            nrm = np.zeros(shape, np.float32) if guides else None
         stats = RenderStatsC()
         _check(lib().wrk_render(self.handle, scene.handle, C.byref(cam), C.byref(p), rgb.ctypes.data,
                                 None if alb is None else alb.ctypes.data, None if nrm is None else nrm.ctypes.data,
